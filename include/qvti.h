@@ -1,0 +1,139 @@
+/* qvti.h -- C ABI of the B200 viscoelastic pseudospectral time stepper.
+ *
+ * Extended, status-returning entry points.  The reference exposes its path
+ * only through the void functions of Myfunctions.h (cuda_Device_malloc,
+ * cuda_Host_initialization, cuda_forward_acoustic_3D, cuda_Device_free);
+ * those are provided unchanged in include/Myfunctions.h and are built on the
+ * functions below.  Each declaration names the reference interface whose
+ * role it takes (file:line within the reference project).
+ *
+ * Conventions (the reference's): fields are float32 [ix][iy][iz], z fastest,
+ * on the total padded grid ntx*nty*ntz with `pml` C-PML cells on each face;
+ * seismograms are [it][ir].  All functions return QVTI_OK (0) or an error
+ * code; qvti_last_error() reports the last failure of the calling process.
+ * Plain pointers and sizes only.
+ */
+#ifndef QVTI_H
+#define QVTI_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    QVTI_OK = 0,
+    QVTI_ERR_ARG = 1,         /* invalid argument                          */
+    QVTI_ERR_CUDA = 2,        /* CUDA runtime error                        */
+    QVTI_ERR_UNSUPPORTED = 3, /* grid size / option not supported          */
+    QVTI_ERR_STATE = 4,       /* call out of order (e.g. no model set)     */
+    QVTI_ERR_OOM = 5,         /* device allocation failed                  */
+    QVTI_ERR_NONFINITE = 6    /* a non-finite value was detected           */
+};
+
+enum { QVTI_SRC_FORCE_X = 0, QVTI_SRC_EXPLOSIVE = 1 };
+
+typedef struct qvti_sim qvti_sim;
+
+typedef struct {
+    int ntx, nty, ntz;  /* total padded grid (PML inside), each even, >= 16, 2/3/5/7-smooth */
+    int pml;            /* C-PML thickness in cells on every face                           */
+    float dx, dy, dz;   /* grid spacing (m)                                                 */
+    float dt;           /* time step (s)                                                    */
+    float f0;           /* reference / source frequency (Hz); w0 = 2 pi f0                   */
+    int vti;            /* 0 isotropic, 1 VTI (Thomsen eps, delta; c66 = c44)               */
+    int device;         /* CUDA device ordinal                                              */
+    float w0;           /* constant-Q reference angular frequency; 0 = 2 pi f0 with the
+                           reference's pi (viscoelas_3D.cpp:109)                              */
+} qvti_config;
+
+/* Device memory the engine needs for a grid (bytes).  Replaces the sizing
+ * implicit in cuda_Device_malloc (cuviscoelas_3D.cu:1689-1916). */
+size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int vti);
+
+/* Allocate a simulation on cfg->device.  Replaces cuda_Device_malloc
+ * (Myfunctions.h:91-96, cuviscoelas_3D.cu:1689-1916). */
+int qvti_create(const qvti_config* cfg, qvti_sim** out);
+
+/* Free everything.  Replaces cuda_Device_free (Myfunctions.h:98-102,
+ * cuviscoelas_3D.cu:1922-2141). */
+int qvti_destroy(qvti_sim* sim);
+
+/* Set the model: velp, vels, rho, gama_p = atan(1/Qp)/pi, gama_s (and eps,
+ * delta when vti) as ntp floats each, host pointers (on_device = 0) or device
+ * pointers (on_device = 1).  Builds the constant-Q, C-PML and k-space tables
+ * in FP64 on the GPU.  Replaces the model H2D copies and the setup kernels of
+ * cuda_forward_acoustic_3D (cuviscoelas_3D.cu:1179-1230). */
+int qvti_set_model(qvti_sim* sim, const float* velp, const float* vels, const float* rho, const float* gama_p,
+                   const float* gama_s, const float* eps, const float* delta, int on_device);
+
+/* Source: type QVTI_SRC_FORCE_X adds wavelet[it] to vx at (s_ix, s_iy, s_iz)
+ * after the stress update of step it (cuviscoelas_3D.cu:772-777);
+ * QVTI_SRC_EXPLOSIVE adds it to pxx, pyy, pzz instead (the reference's
+ * commented explosive variant, cu:775-776).  s_iz is the injection index
+ * itself (the reference-compatible cuda_forward_acoustic_3D adds its +10).
+ * wavelet: nt host floats; nt also sizes the seismogram buffers. */
+int qvti_set_source(qvti_sim* sim, int type, int s_ix, int s_iy, int s_iz, const float* wavelet, int nt);
+
+/* Receivers at depth index r_iz and padded positions (r_ix[i], r_iy[i]),
+ * rn of them, host arrays (cuviscoelas_3D.cu:782-791). */
+int qvti_set_receivers(qvti_sim* sim, int r_iz, const int* r_ix, const int* r_iy, int rn);
+
+/* Zero the wavefield, memory variables and step counter
+ * (cuda_kernel_initialization, cuviscoelas_3D.cu:312-410). */
+int qvti_reset(qvti_sim* sim);
+
+/* Advance nsteps time steps asynchronously (the body of the time loop,
+ * cuviscoelas_3D.cu:1255-1630), replayed from a captured CUDA graph. */
+int qvti_step(qvti_sim* sim, int nsteps);
+
+/* Advance nsteps steps and report their device time in milliseconds,
+ * measured with CUDA events on the simulation's stream (synchronous). */
+int qvti_step_timed(qvti_sim* sim, int nsteps, float* ms);
+
+/* Wait for all queued work. */
+int qvti_sync(qvti_sim* sim);
+
+/* Number of steps advanced since the last reset. */
+int qvti_steps_done(const qvti_sim* sim);
+
+/* Copy the seismograms recorded so far (steps_done x rn each, [it][ir]) to
+ * host memory (cuviscoelas_3D.cu:1640-1645). Any pointer may be NULL. */
+int qvti_get_records(qvti_sim* sim, float* vx, float* vy, float* vz);
+
+/* Copy `count` wavefields starting at `first` in the order
+ * vx vy vz pxx pyy pzz pxy pxz pyz to host memory (count*ntp floats);
+ * snapshots (the reference's dead snapshot block, cu:1611-1627). */
+int qvti_get_fields(qvti_sim* sim, int first, int count, float* out);
+
+/* Device pointer of wavefield `which` (same order) for in-HBM consumers. */
+int qvti_device_field(qvti_sim* sim, int which, float** dev_ptr);
+
+/* Sum of squares of every wavefield (FP64 reduction on the device): the
+ * per-run energy-norm check; also flags non-finite values. */
+int qvti_field_norms(qvti_sim* sim, double* norms9, int* nonfinite);
+
+/* One whole shot with host buffers, synchronous: model upload, setup,
+ * nt steps, seismogram download.  The reference-call semantics of
+ * cuda_forward_acoustic_3D (Myfunctions.h:77-85, cuviscoelas_3D.cu:1137-1652)
+ * with an explicit injection index. rec_* receive nt*rn floats each. */
+int qvti_forward_shot(qvti_sim* sim, const float* velp, const float* vels, const float* rho, const float* gama_p,
+                      const float* gama_s, const float* eps, const float* delta, int src_type, int s_ix, int s_iy,
+                      int s_iz, const float* wavelet, int nt, int r_iz, const int* r_ix, const int* r_iy, int rn,
+                      float* rec_vx, float* rec_vy, float* rec_vz);
+
+/* 1D staggered spectral derivative of a host field along `axis` (0 x, 1 y,
+ * 2 z) with the forward (fwd=1, i k e^{+ik d/2}) or backward shift; the
+ * building block of the velocity update (cuviscoelas_3D.cu:707-744 with the
+ * transforms it feeds).  For tests and diagnostics. */
+int qvti_derivative_1d(qvti_sim* sim, int axis, int fwd, const float* in, float* out);
+
+/* Last error code of this process and its description. */
+int qvti_last_error(void);
+const char* qvti_error_string(int code);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,600 @@
+// Host side of the engine: allocation, FP64 setup on the GPU, CUDA-graph
+// replay of the step, and the qvti_* C ABI (include/qvti.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <vector>
+
+#include "engine.cuh"
+#include "../../include/qvti.h"
+
+namespace qvti {
+namespace {
+
+thread_local int g_last_error = QVTI_OK;
+std::mutex g_err_mu;
+int g_last_error_global = QVTI_OK;
+
+int fail(int code)
+{
+    g_last_error = code;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_last_error_global = code;
+    return code;
+}
+
+#define QV_CUDA(call)                                                                        \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            fprintf(stderr, "qvti: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), \
+                    __FILE__, __LINE__);                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? QVTI_ERR_OOM : QVTI_ERR_CUDA);     \
+        }                                                                                    \
+    } while (0)
+
+bool smooth(int n)
+{
+    for (int r : {2, 3, 5, 7})
+        while (n % r == 0) n /= r;
+    return n == 1;
+}
+
+// Radix schedule: radix 8 first, then 4, 2, and the odd radices.
+bool make_plan(int n, FftPlan* p)
+{
+    p->n = n;
+    p->nst = 0;
+    int m = n;
+    while (m % 8 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 8; m /= 8; }
+    while (m % 4 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 4; m /= 4; }
+    while (m % 2 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 2; m /= 2; }
+    for (int r : {3, 5, 7})
+        while (m % r == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = r; m /= r; }
+    if (m != 1) return false;
+    if (p->nst < 2) return false;
+    return true;
+}
+
+// FP64 construction of the 1D tables of one axis on the GPU:
+// twiddles e^{-2 pi i k/n}; |k| (cuviscoelas_3D.cu:54-67); staggered-shift
+// multipliers i k e^{+-i k d/2} (cu:76-151) with the Nyquist bin reduced to
+// its real part -- the Hermitian part of the multiplier, which is what the
+// real part of the reference's C2C output sees; C-PML a, b (cu:213-309,
+// velp_max forced to 5000, R = 1e-2, pi = 3.1415926) and their half-point
+// averages 0.5 (v[i] + v[i+1]).
+__global__ void k_axis_tables(int n, double d, double f0, int pml, float2* tw, float* kmag, float2* F, float2* B,
+                              float* a, float* b, float* ah, float* bh)
+{
+    const double pi_ref = 3.1415926;
+    for (int i = threadIdx.x + blockIdx.x * blockDim.x; i < n; i += blockDim.x * gridDim.x) {
+        double s, c;
+        sincospi(-2.0 * i / n, &s, &c);
+        tw[i] = make_float2((float)c, (float)s);
+        const int m = i <= n / 2 ? i : n - i;
+        const double tmp = 2.0 * pi_ref / n / d;
+        kmag[i] = (float)(tmp * m);
+        const double sn = sin(m * pi_ref / n), cs = cos(m * pi_ref / n);
+        double fr, fi, br, bi;
+        if (i <= n / 2) { fr = -tmp * m * sn; fi = tmp * m * cs; br = tmp * m * sn; bi = tmp * m * cs; }
+        else            { fr = -tmp * m * sn; fi = -tmp * m * cs; br = tmp * m * sn; bi = -tmp * m * cs; }
+        if (2 * i == n) { fi = 0.0; bi = 0.0; }
+        F[i] = make_float2((float)fr, (float)fi);
+        B[i] = make_float2((float)br, (float)bi);
+        auto prof = [&](int j, double* av, double* bv) {
+            const double alpha_max = pi_ref * f0;
+            const double om_max = 4.0 * 5000.0 * log(1.0 / (double)1e-2f) / (2.0 * pml * d);
+            int jj = j < pml ? j : (j >= n - pml ? n - 1 - j : -1);
+            if (jj < 0) { *av = alpha_max; *bv = 0.0; return; }
+            const double al = alpha_max * pow((double)jj / (pml - 1), 2.0);
+            const double om = om_max * pow((double)(pml - 1 - jj) / pml, 3.0);
+            *av = al + om;
+            *bv = om;
+        };
+        double a0, b0, a1, b1;
+        prof(i, &a0, &b0);
+        prof(i + 1 < n ? i + 1 : i, &a1, &b1);
+        a[i] = (float)a0;
+        b[i] = (float)b0;
+        ah[i] = (float)(0.5 * (a0 + a1));
+        bh[i] = (float)(0.5 * (b0 + b1));
+    }
+}
+
+__global__ void k_norms(long long ntp, const float* f, double* out, int* nonfinite)
+{
+    double acc = 0.0;
+    int bad = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntp; i += (long long)gridDim.x * blockDim.x) {
+        const float v = f[i];
+        if (!isfinite(v)) bad = 1;
+        else acc += (double)v * v;
+    }
+    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    __shared__ double red[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = acc;
+    bad = __syncthreads_or(bad);
+    if (w == 0) {
+        acc = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) atomicAdd(out, acc);
+    }
+    if (threadIdx.x == 0 && bad) atomicOr(nonfinite, 1);
+}
+
+}  // namespace
+
+struct Sim {
+    qvti_config cfg{};
+    int nx = 0, ny = 0, nz = 0, nkz = 0;
+    long long ntp = 0;
+    cudaStream_t st = nullptr;
+    KP kp{};
+    std::vector<void*> allocs;
+    float* coef[25] = {};
+    int* d_it = nullptr;
+    float* d_rik = nullptr;
+    int* d_rix = nullptr;
+    int* d_riy = nullptr;
+    float* d_rec[3] = {};
+    double* d_norm = nullptr;
+    int* d_bad = nullptr;
+    int nt = 0, rn = 0;
+    bool have_model = false, have_src = false;
+    int steps = 0;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    template <class T>
+    int alloc(T** p, size_t count)
+    {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+        if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? QVTI_ERR_OOM : QVTI_ERR_CUDA);
+        allocs.push_back(q);
+        *p = static_cast<T*>(q);
+        return QVTI_OK;
+    }
+    void release(void* p)
+    {
+        for (auto& q : allocs)
+            if (q == p) { cudaFree(q); q = nullptr; }
+    }
+    ~Sim()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        for (void* p : allocs)
+            if (p) cudaFree(p);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+
+// Number of full-grid float arrays and half-spectrum complex arrays.
+constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 25 + 5 + 3;
+constexpr int kSpecArrays = 3 + kNumG;
+
+int build_graph(Sim* s)
+{
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    cudaGraph_t g = nullptr;
+    QV_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+    launch_step(s->kp, s->st);
+    QV_CUDA(cudaStreamEndCapture(s->st, &g));
+    cudaError_t e = cudaGraphInstantiate(&s->gexec, g, 0);
+    cudaGraphDestroy(g);
+    QV_CUDA(e);
+    return QVTI_OK;
+}
+
+}  // namespace
+}  // namespace qvti
+
+using qvti::Sim;
+using qvti::fail;
+
+struct qvti_sim : qvti::Sim {};
+
+extern "C" size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int vti)
+{
+    (void)vti;
+    const size_t ntp = (size_t)ntx * nty * ntz;
+    const size_t nspec = (size_t)(ntz / 2 + 1) * ntx * nty;
+    return ntp * sizeof(float) * qvti::kRealArrays + nspec * sizeof(float2) * qvti::kSpecArrays;
+}
+
+extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
+{
+    using namespace qvti;
+    if (!cfg || !out) return fail(QVTI_ERR_ARG);
+    *out = nullptr;
+    const int nx = cfg->ntx, ny = cfg->nty, nz = cfg->ntz;
+    if (nx < 16 || ny < 16 || nz < 16 || nx > 1024 || ny > 1024 || nz > 1024) return fail(QVTI_ERR_UNSUPPORTED);
+    if ((nx | ny | nz) & 1) return fail(QVTI_ERR_UNSUPPORTED);
+    if (!smooth(nx) || !smooth(ny) || !smooth(nz)) return fail(QVTI_ERR_UNSUPPORTED);
+    if (cfg->pml < 2 || 2 * cfg->pml >= nx || 2 * cfg->pml >= ny || 2 * cfg->pml >= nz) return fail(QVTI_ERR_ARG);
+    if (!(cfg->dx > 0 && cfg->dy > 0 && cfg->dz > 0 && cfg->dt > 0 && cfg->f0 > 0)) return fail(QVTI_ERR_ARG);
+    FftPlan px, py, pz;
+    if (!make_plan(nx, &px) || !make_plan(ny, &py) || !make_plan(nz, &pz)) return fail(QVTI_ERR_UNSUPPORTED);
+
+    QV_CUDA(cudaSetDevice(cfg->device));
+    static std::once_flag once;
+    static int cfg_err = 0;
+    std::call_once(once, [] { cfg_err = configure_kernels(); });
+    if (cfg_err) return fail(QVTI_ERR_CUDA);
+
+    Sim* s = new (std::nothrow) qvti_sim();
+    if (!s) return fail(QVTI_ERR_OOM);
+    s->cfg = *cfg;
+    s->nx = nx; s->ny = ny; s->nz = nz; s->nkz = nz / 2 + 1;
+    s->ntp = (long long)nx * ny * nz;
+    auto bail = [&](int code) { delete s; return fail(code); };
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) return bail(QVTI_ERR_CUDA);
+    if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) return bail(QVTI_ERR_CUDA);
+
+    KP& k = s->kp;
+    k.nx = nx; k.ny = ny; k.nz = nz; k.nkz = s->nkz; k.pml = cfg->pml;
+    k.ntp = s->ntp;
+    k.dt = cfg->dt;
+    k.inv_ntp = (float)(1.0 / (double)s->ntp);
+    k.px = px; k.py = py; k.pz = pz;
+    const long long ntp = s->ntp, nspec = (long long)s->nkz * nx * ny;
+
+    // 1D tables
+    float2 *twx, *twy, *twz, *Fx, *Bx, *Fy, *By, *Fz, *Bz;
+    float *kx, *ky, *kz, *t[12];
+    int rc = 0;
+    rc |= s->alloc(&twx, nx); rc |= s->alloc(&twy, ny); rc |= s->alloc(&twz, nz);
+    rc |= s->alloc(&Fx, nx); rc |= s->alloc(&Bx, nx); rc |= s->alloc(&Fy, ny); rc |= s->alloc(&By, ny);
+    rc |= s->alloc(&Fz, nz); rc |= s->alloc(&Bz, nz);
+    rc |= s->alloc(&kx, nx); rc |= s->alloc(&ky, ny); rc |= s->alloc(&kz, nz);
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 4; ++j) rc |= s->alloc(&t[a * 4 + j], a == 0 ? nx : a == 1 ? ny : nz);
+    if (rc) return bail(g_last_error);
+    k.tw_x = twx; k.tw_y = twy; k.tw_z = twz;
+    k.Fx = Fx; k.Bx = Bx; k.Fy = Fy; k.By = By; k.Fz = Fz; k.Bz = Bz;
+    k.kx = kx; k.ky = ky; k.kz = kz;
+    k.ax = t[0]; k.bx = t[1]; k.axh = t[2]; k.bxh = t[3];
+    k.ay = t[4]; k.by = t[5]; k.ayh = t[6]; k.byh = t[7];
+    k.az = t[8]; k.bz = t[9]; k.azh = t[10]; k.bzh = t[11];
+    k_axis_tables<<<4, 256, 0, s->st>>>(nx, cfg->dx, cfg->f0, cfg->pml, twx, kx, Fx, Bx, t[0], t[1], t[2], t[3]);
+    k_axis_tables<<<4, 256, 0, s->st>>>(ny, cfg->dy, cfg->f0, cfg->pml, twy, ky, Fy, By, t[4], t[5], t[6], t[7]);
+    k_axis_tables<<<4, 256, 0, s->st>>>(nz, cfg->dz, cfg->f0, cfg->pml, twz, kz, Fz, Bz, t[8], t[9], t[10], t[11]);
+
+    // full-grid arrays
+    for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.v[c], ntp);
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.s[c], ntp);
+    for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.R[c], ntp);
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.Q[c], ntp);
+    for (int c = 0; c < 9; ++c) rc |= s->alloc(&k.php[c], ntp);
+    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.phn[c], ntp);
+    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.qn[c], ntp);
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.phs[c], ntp);
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.qs[c], ntp);
+    if (rc) return bail(g_last_error);
+    float* mu[5];
+    float* rinv[3];
+    for (int c = 0; c < 5; ++c) rc |= s->alloc(&mu[c], ntp);
+    for (int c = 0; c < 3; ++c) rc |= s->alloc(&rinv[c], ntp);
+    for (int c = 0; c < 25; ++c) rc |= s->alloc(&s->coef[c], ntp);
+    for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.H[c], nspec);
+    for (int c = 0; c < kNumG; ++c) rc |= s->alloc(&k.G[c], nspec);
+    rc |= s->alloc(&s->d_it, 1);
+    rc |= s->alloc(&s->d_norm, 16);
+    rc |= s->alloc(&s->d_bad, 4);
+    if (rc) return bail(g_last_error);
+    for (int j = 0; j < 5; ++j) {
+        k.MU[j] = mu[j];
+        k.K11[j] = s->coef[j];
+        k.K12[j] = s->coef[5 + j];
+        k.K13[j] = s->coef[10 + j];
+        k.K33[j] = s->coef[15 + j];
+    }
+    for (int c = 0; c < 3; ++c) k.rinv[c] = rinv[c];
+    k.d_it = s->d_it;
+    k.src_type = 0; k.s_ix = -1; k.s_iy = 0; k.s_iz = 0;
+    k.rik = nullptr; k.nt_rec = 0; k.rn = 0; k.r_iz = 0; k.r_ix = nullptr; k.r_iy = nullptr;
+    for (int c = 0; c < 3; ++c) k.rec[c] = nullptr;
+    if (cudaStreamSynchronize(s->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return bail(QVTI_ERR_CUDA);
+    *out = static_cast<qvti_sim*>(s);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_destroy(qvti_sim* sim)
+{
+    if (!sim) return fail(QVTI_ERR_ARG);
+    cudaSetDevice(sim->cfg.device);
+    cudaStreamSynchronize(sim->st);
+    delete sim;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels, const float* rho, const float* gama_p,
+                              const float* gama_s, const float* eps, const float* delta, int on_device)
+{
+    using namespace qvti;
+    if (!s || !velp || !vels || !rho || !gama_p || !gama_s) return fail(QVTI_ERR_ARG);
+    if (s->cfg.vti && (!eps || !delta)) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    const long long ntp = s->ntp;
+    const size_t bytes = sizeof(float) * ntp;
+    const int nin = s->cfg.vti ? 7 : 5;
+    const float* host[7] = {velp, vels, rho, gama_p, gama_s, eps, delta};
+    const float* dev[7] = {};
+    float* tmp[7] = {};
+    if (on_device) {
+        for (int i = 0; i < nin; ++i) dev[i] = host[i];
+    } else {
+        for (int i = 0; i < nin; ++i) {
+            if (s->alloc(&tmp[i], ntp)) return g_last_error;
+            QV_CUDA(cudaMemcpyAsync(tmp[i], host[i], bytes, cudaMemcpyHostToDevice, s->st));
+            dev[i] = tmp[i];
+        }
+    }
+    float** d_coef = nullptr;
+    QV_CUDA(cudaMalloc(&d_coef, sizeof(float*) * 25));
+    QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 25, cudaMemcpyHostToDevice, s->st));
+    const float w0 = s->cfg.w0 > 0 ? s->cfg.w0 : (float)(2 * 3.1415926 * s->cfg.f0);  // viscoelas_3D.cpp:109
+    launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
+                      s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, w0, d_coef, s->st);
+    launch_mu_rinv(s->kp, dev[2], s->coef + 20, s->st);
+    QV_CUDA(cudaGetLastError());
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    cudaFree(d_coef);
+    for (int i = 0; i < nin; ++i)
+        if (tmp[i]) s->release(tmp[i]);
+    s->have_model = true;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_iz, const float* wavelet, int nt)
+{
+    using namespace qvti;
+    if (!s || !wavelet || nt <= 0 || (type != QVTI_SRC_FORCE_X && type != QVTI_SRC_EXPLOSIVE)) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    if (s->d_rik) { s->release(s->d_rik); s->d_rik = nullptr; }
+    for (int c = 0; c < 3; ++c)
+        if (s->d_rec[c]) { s->release(s->d_rec[c]); s->d_rec[c] = nullptr; }
+    if (s->alloc(&s->d_rik, nt)) return g_last_error;
+    QV_CUDA(cudaMemcpy(s->d_rik, wavelet, sizeof(float) * nt, cudaMemcpyHostToDevice));
+    s->nt = nt;
+    KP& k = s->kp;
+    k.src_type = type;
+    const bool inside = s_ix >= 0 && s_ix < s->nx && s_iy >= 0 && s_iy < s->ny && s_iz >= 0 && s_iz < s->nz;
+    k.s_ix = inside ? s_ix : -1;
+    k.s_iy = s_iy;
+    k.s_iz = s_iz;
+    k.rik = s->d_rik;
+    k.nt_rec = nt;
+    if (s->rn > 0)
+        for (int c = 0; c < 3; ++c) {
+            if (s->alloc(&s->d_rec[c], (size_t)nt * s->rn)) return g_last_error;
+            QV_CUDA(cudaMemset(s->d_rec[c], 0, sizeof(float) * (size_t)nt * s->rn));
+            k.rec[c] = s->d_rec[c];
+        }
+    s->have_src = true;
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const int* r_iy, int rn)
+{
+    using namespace qvti;
+    if (!s || rn < 0 || (rn > 0 && (!r_ix || !r_iy)) || r_iz < 0 || r_iz >= s->nz) return fail(QVTI_ERR_ARG);
+    for (int i = 0; i < rn; ++i)
+        if (r_ix[i] < 0 || r_ix[i] >= s->nx || r_iy[i] < 0 || r_iy[i] >= s->ny) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    if (s->d_rix) { s->release(s->d_rix); s->d_rix = nullptr; }
+    if (s->d_riy) { s->release(s->d_riy); s->d_riy = nullptr; }
+    for (int c = 0; c < 3; ++c)
+        if (s->d_rec[c]) { s->release(s->d_rec[c]); s->d_rec[c] = nullptr; }
+    KP& k = s->kp;
+    s->rn = rn;
+    k.rn = rn;
+    k.r_iz = r_iz;
+    if (rn > 0) {
+        if (s->alloc(&s->d_rix, rn) || s->alloc(&s->d_riy, rn)) return g_last_error;
+        QV_CUDA(cudaMemcpy(s->d_rix, r_ix, sizeof(int) * rn, cudaMemcpyHostToDevice));
+        QV_CUDA(cudaMemcpy(s->d_riy, r_iy, sizeof(int) * rn, cudaMemcpyHostToDevice));
+    }
+    k.r_ix = s->d_rix;
+    k.r_iy = s->d_riy;
+    for (int c = 0; c < 3; ++c) k.rec[c] = nullptr;
+    if (rn > 0 && s->nt > 0)
+        for (int c = 0; c < 3; ++c) {
+            if (s->alloc(&s->d_rec[c], (size_t)s->nt * rn)) return g_last_error;
+            QV_CUDA(cudaMemset(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * rn));
+            k.rec[c] = s->d_rec[c];
+        }
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_reset(qvti_sim* s)
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    KP& k = s->kp;
+    const size_t b = sizeof(float) * s->ntp;
+    for (int c = 0; c < 3; ++c) QV_CUDA(cudaMemsetAsync(k.v[c], 0, b, s->st));
+    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.s[c], 0, b, s->st));
+    for (int c = 0; c < 3; ++c) QV_CUDA(cudaMemsetAsync(k.R[c], 0, b, s->st));
+    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.Q[c], 0, b, s->st));
+    for (int c = 0; c < 9; ++c) QV_CUDA(cudaMemsetAsync(k.php[c], 0, b, s->st));
+    for (int c = 0; c < 8; ++c) QV_CUDA(cudaMemsetAsync(k.phn[c], 0, b, s->st));
+    for (int c = 0; c < 8; ++c) QV_CUDA(cudaMemsetAsync(k.qn[c], 0, b, s->st));
+    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.phs[c], 0, b, s->st));
+    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.qs[c], 0, b, s->st));
+    const int minus1 = -1;
+    QV_CUDA(cudaMemcpyAsync(s->d_it, &minus1, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    for (int c = 0; c < 3; ++c)
+        if (s->d_rec[c]) QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * s->rn, s->st));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    s->steps = 0;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_step(qvti_sim* s, int nsteps)
+{
+    using namespace qvti;
+    if (!s || nsteps < 0) return fail(QVTI_ERR_ARG);
+    if (!s->have_model || !s->have_src) return fail(QVTI_ERR_STATE);
+    if (s->steps + nsteps > s->nt) return fail(QVTI_ERR_ARG);  // wavelet / record capacity
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    if (!s->gexec) {
+        int rc = build_graph(s);
+        if (rc) return rc;
+    }
+    for (int i = 0; i < nsteps; ++i) QV_CUDA(cudaGraphLaunch(s->gexec, s->st));
+    s->steps += nsteps;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_step_timed(qvti_sim* s, int nsteps, float* ms)
+{
+    using namespace qvti;
+    if (!s || !ms) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    if (!s->gexec && s->have_model && s->have_src) {
+        int rc = build_graph(s);
+        if (rc) return rc;
+    }
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    QV_CUDA(cudaEventRecord(s->ev0, s->st));
+    int rc = qvti_step(s, nsteps);
+    if (rc) return rc;
+    QV_CUDA(cudaEventRecord(s->ev1, s->st));
+    QV_CUDA(cudaEventSynchronize(s->ev1));
+    QV_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+    return QVTI_OK;
+}
+
+extern "C" int qvti_sync(qvti_sim* s)
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    return QVTI_OK;
+}
+
+extern "C" int qvti_steps_done(const qvti_sim* s) { return s ? s->steps : -1; }
+
+extern "C" int qvti_get_records(qvti_sim* s, float* vx, float* vy, float* vz)
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    float* dst[3] = {vx, vy, vz};
+    const size_t n = (size_t)s->steps * s->rn;
+    for (int c = 0; c < 3; ++c)
+        if (dst[c] && n && s->d_rec[c]) QV_CUDA(cudaMemcpy(dst[c], s->d_rec[c], n * sizeof(float), cudaMemcpyDeviceToHost));
+    return QVTI_OK;
+}
+
+static float* field_ptr(qvti_sim* s, int which)
+{
+    if (which < 3) return s->kp.v[which];
+    static const int smap[6] = {0, 1, 2, 3, 4, 5};  // pxx pyy pzz pxy pxz pyz
+    return s->kp.s[smap[which - 3]];
+}
+
+extern "C" int qvti_get_fields(qvti_sim* s, int first, int count, float* out)
+{
+    using namespace qvti;
+    if (!s || !out || first < 0 || count < 0 || first + count > 9) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    for (int f = 0; f < count; ++f)
+        QV_CUDA(cudaMemcpy(out + (size_t)f * s->ntp, field_ptr(s, first + f), sizeof(float) * s->ntp,
+                           cudaMemcpyDeviceToHost));
+    return QVTI_OK;
+}
+
+extern "C" int qvti_device_field(qvti_sim* s, int which, float** p)
+{
+    if (!s || !p || which < 0 || which > 8) return qvti::fail(QVTI_ERR_ARG);
+    *p = field_ptr(s, which);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_field_norms(qvti_sim* s, double* norms9, int* nonfinite)
+{
+    using namespace qvti;
+    if (!s || !norms9) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    int bad_all = 0;
+    for (int f = 0; f < 9; ++f) {
+        QV_CUDA(cudaMemsetAsync(s->d_norm, 0, sizeof(double), s->st));
+        QV_CUDA(cudaMemsetAsync(s->d_bad, 0, sizeof(int), s->st));
+        k_norms<<<148 * 4, 256, 0, s->st>>>(s->ntp, field_ptr(s, f), s->d_norm, s->d_bad);
+        double acc = 0;
+        int bad = 0;
+        QV_CUDA(cudaMemcpyAsync(&acc, s->d_norm, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+        QV_CUDA(cudaMemcpyAsync(&bad, s->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+        QV_CUDA(cudaStreamSynchronize(s->st));
+        norms9[f] = acc;
+        bad_all |= bad;
+    }
+    if (nonfinite) *nonfinite = bad_all;
+    return bad_all ? fail(QVTI_ERR_NONFINITE) : QVTI_OK;
+}
+
+extern "C" int qvti_forward_shot(qvti_sim* s, const float* velp, const float* vels, const float* rho,
+                                 const float* gama_p, const float* gama_s, const float* eps, const float* delta,
+                                 int src_type, int s_ix, int s_iy, int s_iz, const float* wavelet, int nt, int r_iz,
+                                 const int* r_ix, const int* r_iy, int rn, float* rec_vx, float* rec_vy, float* rec_vz)
+{
+    int rc;
+    if ((rc = qvti_set_model(s, velp, vels, rho, gama_p, gama_s, eps, delta, 0))) return rc;
+    if ((rc = qvti_set_receivers(s, r_iz, r_ix, r_iy, rn))) return rc;
+    if ((rc = qvti_set_source(s, src_type, s_ix, s_iy, s_iz, wavelet, nt))) return rc;
+    if ((rc = qvti_reset(s))) return rc;
+    if ((rc = qvti_step(s, nt))) return rc;
+    return qvti_get_records(s, rec_vx, rec_vy, rec_vz);
+}
+
+extern "C" int qvti_derivative_1d(qvti_sim* s, int axis, int fwd, const float* in, float* out)
+{
+    using namespace qvti;
+    if (!s || !in || !out || axis < 0 || axis > 2) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    float *din = nullptr, *dout = nullptr;
+    const size_t b = sizeof(float) * s->ntp;
+    QV_CUDA(cudaMalloc(&din, b));
+    QV_CUDA(cudaMalloc(&dout, b));
+    QV_CUDA(cudaMemcpy(din, in, b, cudaMemcpyHostToDevice));
+    launch_derivative_1d(s->kp, axis, fwd, din, dout, s->st);
+    QV_CUDA(cudaGetLastError());
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    QV_CUDA(cudaMemcpy(out, dout, b, cudaMemcpyDeviceToHost));
+    cudaFree(din);
+    cudaFree(dout);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_last_error(void) { return qvti::g_last_error; }
+
+extern "C" const char* qvti_error_string(int code)
+{
+    switch (code) {
+        case QVTI_OK: return "ok";
+        case QVTI_ERR_ARG: return "invalid argument";
+        case QVTI_ERR_CUDA: return "CUDA runtime error";
+        case QVTI_ERR_UNSUPPORTED: return "unsupported grid size or option";
+        case QVTI_ERR_STATE: return "call out of order";
+        case QVTI_ERR_OOM: return "device allocation failed";
+        case QVTI_ERR_NONFINITE: return "non-finite value detected";
+        default: return "unknown error";
+    }
+}

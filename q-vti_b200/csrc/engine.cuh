@@ -1,0 +1,86 @@
+// Shared declarations of the B200 viscoelastic pseudospectral engine.
+//
+// Layout in HBM (one shot, total padded grid nx*ny*nz, z fastest exactly as
+// the reference's ip = ix*nty*ntz + iy*ntz + iz, cuviscoelas_3D.cu:176):
+//
+//   state      v[3], s[6]  (vx vy vz; sxx syy szz sxy sxz syz)      float
+//   R[3]       partial right-hand side of the velocity update: the z and y
+//              stress derivatives (+ their C-PML memory terms), finished by
+//              the x-pencil kernel                                   float
+//   Q[6]       loss potentials: sum over terms of tau-coefficient x the
+//              |k|^-1 and |k|^0 dispersion fields of the previous step; the
+//              reference's spectral time derivative (V - Vprev)/dt
+//              (cuviscoelas_3D.cu:514-531) becomes (Q - Qprev)/dt by
+//              linearity, saving 18 of its 45 inverse transforms    float
+//   C-PML      memory variables and per-term loss potentials, allocated
+//              full size but read/written only inside their axis slab
+//              (they are identically zero elsewhere, b = 0 there)   float
+//   coef       K11 K12 K13 K33 (5 each: eta1 eta2 eta3 tau1 tau2), MU (5,
+//              8-point averaged shear set), 1/rho-bar per velocity component;
+//              built once per shot in FP64 and rounded              float
+//   H[3]       velocity spectra, half along z: [kz][x][y], nkz = nz/2+1 float2
+//   G[27]      9 directional derivatives x 3 dispersion operators
+//              (|k|^-1, 1, |k|) of the velocity spectra, [kz][x][y] float2
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "fft.cuh"
+
+namespace qvti {
+
+constexpr int kNumG = 27;
+
+struct KP {
+    int nx, ny, nz, nkz, pml;
+    long long ntp;
+    float dt, inv_ntp;
+    FftPlan px, py, pz;
+    // 1D tables (device)
+    const float2 *tw_x, *tw_y, *tw_z;             // e^{-2 pi i k/n}
+    const float2 *Fx, *Bx, *Fy, *By, *Fz, *Bz;    // staggered-shift derivative multipliers (Nyquist bin real)
+    const float *kx, *ky, *kz;                    // |k| per index
+    const float *ax, *bx, *axh, *bxh;             // C-PML a, b and their half-point averages
+    const float *ay, *by, *ayh, *byh;
+    const float *az, *bz, *azh, *bzh;
+    // state
+    float* v[3];
+    float* s[6];
+    float* R[3];
+    float* Q[6];
+    float* php[9];   // velocity-side memory variables, reference order (cu:1049-1074)
+    float* phn[8];   // normal-stress memory variables: x_xx x_xy x_xz y_yx y_yy y_yz z_zxy z_zz
+    float* qn[8];    // matching per-term loss potentials
+    float* phs[6];   // shear memory variables: vx_z vz_x vx_y vy_x vy_z vz_y
+    float* qs[6];
+    // coefficients
+    const float* K11[5];
+    const float* K12[5];
+    const float* K13[5];
+    const float* K33[5];
+    const float* MU[5];
+    const float* rinv[3];
+    // spectra
+    float2* H[3];
+    float2* G[kNumG];
+    // source and receivers
+    int src_type, s_ix, s_iy, s_iz;
+    const float* rik;
+    int nt_rec, rn, r_iz;
+    const int *r_ix, *r_iy;
+    float* rec[3];
+    int* d_it;       // current step index, advanced on the device each step
+};
+
+// Host-side launchers (step_kernels.cu).  All launch on `st`.
+void launch_step(const KP& kp, cudaStream_t st);
+void launch_coef_build(const KP& kp, const float* velp, const float* vels, const float* rho,
+                       const float* gp, const float* gs, const float* eps, const float* delta, int vti,
+                       float w0, float* const* coef_out, cudaStream_t st);
+void launch_mu_rinv(const KP& kp, const float* rho, const float* const* sset, cudaStream_t st);
+int configure_kernels();   // raise dynamic shared-memory limits, returns cudaError_t
+
+// Individual stages, exposed for unit tests through the C ABI.
+void launch_derivative_1d(const KP& kp, int axis, int fwd_shift, const float* in, float* out, cudaStream_t st);
+
+}  // namespace qvti

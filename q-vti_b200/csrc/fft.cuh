@@ -1,0 +1,254 @@
+// Shared-memory mixed-radix FFT building blocks for sm_100a.
+//
+// The spectral-derivative engine replaces the reference's 63 cuFFT C2C calls
+// per step (cuviscoelas_3D.cu:1272-1562) with pencil kernels that transform a
+// tile of P pencils of one axis on chip.  A transform of length n = prod(rad)
+// runs as a Stockham autosort sequence of radix-2/3/4/5/7/8 stages:
+//
+//   * stage 0 reads its inputs through a caller-supplied `load(p, i)` functor
+//     (straight from global memory, or from shared memory with a k-space
+//     multiplier applied on the fly),
+//   * middle stages ping-pong between two shared-memory buffers,
+//   * the last stage hands its outputs to a `store(p, i, v)` functor (to global
+//     memory, or into an update epilogue).
+//
+// so a pencil costs one trip through HBM no matter how many stages it has.
+// Element (p, i) of a pencil tile lives at buf[p*ps + i*is]; the thread
+// mapping is pencil-fastest (PF) when pencils are contiguous in global memory
+// and index-fastest otherwise, so both the global and the shared-memory
+// accesses of every stage are coalesced / bank-spread.
+//
+// Convention: forward e^{-2 pi i k m / n}, inverse e^{+...}, unnormalised,
+// matching cuFFT's CUFFT_FORWARD / CUFFT_INVERSE used by the reference.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace qvti {
+
+constexpr int kMaxStages = 12;
+
+struct FftPlan {
+    int n;                   // transform length
+    int nst;                 // number of stages (>= 2)
+    int rad[kMaxStages];     // radix of each stage, first stage first
+};
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b)  // a * conj(b)
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse)
+__device__ __forceinline__ float2 rot(float2 a, bool inv) { return inv ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x); }
+
+// ---------------------------------------------------------------- radix DFTs
+template <int R>
+struct Dft;
+
+template <>
+struct Dft<2> {
+    static __device__ __forceinline__ void run(float2* v, bool)
+    {
+        float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <>
+struct Dft<4> {
+    static __device__ __forceinline__ void run(float2* v, bool inv)
+    {
+        float2 s0 = cadd(v[0], v[2]), s1 = csub(v[0], v[2]);
+        float2 s2 = cadd(v[1], v[3]), s3 = rot(csub(v[1], v[3]), inv);
+        v[0] = cadd(s0, s2);
+        v[2] = csub(s0, s2);
+        v[1] = cadd(s1, s3);
+        v[3] = csub(s1, s3);
+    }
+};
+
+template <>
+struct Dft<8> {
+    static __device__ __forceinline__ void run(float2* v, bool inv)
+    {
+        const float c = 0.70710678118654752f;
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4>::run(e, inv);
+        Dft<4>::run(o, inv);
+        // o[k] *= W8^k  (W8 = e^{-i pi/4} forward, conjugate inverse)
+        float2 t1 = inv ? make_float2(c * (o[1].x - o[1].y), c * (o[1].x + o[1].y))
+                        : make_float2(c * (o[1].x + o[1].y), c * (o[1].y - o[1].x));
+        float2 t2 = rot(o[2], inv);
+        float2 t3 = inv ? make_float2(-c * (o[3].x + o[3].y), c * (o[3].x - o[3].y))
+                        : make_float2(c * (o[3].y - o[3].x), -c * (o[3].x + o[3].y));
+        v[0] = cadd(e[0], o[0]);
+        v[4] = csub(e[0], o[0]);
+        v[1] = cadd(e[1], t1);
+        v[5] = csub(e[1], t1);
+        v[2] = cadd(e[2], t2);
+        v[6] = csub(e[2], t2);
+        v[3] = cadd(e[3], t3);
+        v[7] = csub(e[3], t3);
+    }
+};
+
+// Odd radices: direct DFT with the roots of unity cos/sin(2 pi k / R).
+template <int R>
+struct OddRoots;
+template <>
+struct OddRoots<3> {
+    static __device__ __forceinline__ float c(int k) { return k == 0 ? 1.f : -0.5f; }
+    static __device__ __forceinline__ float s(int k) { return k == 0 ? 0.f : (k == 1 ? 0.866025404f : -0.866025404f); }
+};
+template <>
+struct OddRoots<5> {
+    static __device__ __forceinline__ float c(int k)
+    {
+        return k == 0 ? 1.f : (k == 1 || k == 4) ? 0.309016994f : -0.809016994f;
+    }
+    static __device__ __forceinline__ float s(int k)
+    {
+        return k == 0 ? 0.f : k == 1 ? 0.951056516f : k == 2 ? 0.587785252f : k == 3 ? -0.587785252f : -0.951056516f;
+    }
+};
+template <>
+struct OddRoots<7> {
+    static __device__ __forceinline__ float c(int k)
+    {
+        return k == 0 ? 1.f : (k == 1 || k == 6) ? 0.623489802f : (k == 2 || k == 5) ? -0.222520934f : -0.900968868f;
+    }
+    static __device__ __forceinline__ float s(int k)
+    {
+        return k == 0 ? 0.f : k == 1 ? 0.781831482f : k == 2 ? 0.974927912f : k == 3 ? 0.433883739f
+             : k == 4 ? -0.433883739f : k == 5 ? -0.974927912f : -0.781831482f;
+    }
+};
+
+template <int R>
+struct DftOdd {
+    static __device__ __forceinline__ void run(float2* v, bool inv)
+    {
+        float2 out[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            float2 acc = v[0];
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const int k = (q * r) % R;
+                const float c = OddRoots<R>::c(k);
+                const float s = inv ? OddRoots<R>::s(k) : -OddRoots<R>::s(k);
+                acc.x += v[r].x * c - v[r].y * s;
+                acc.y += v[r].x * s + v[r].y * c;
+            }
+            out[q] = acc;
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = out[q];
+    }
+};
+template <>
+struct Dft<3> : DftOdd<3> {};
+template <>
+struct Dft<5> : DftOdd<5> {};
+template <>
+struct Dft<7> : DftOdd<7> {};
+
+// ------------------------------------------------------------------- stages
+template <int R, bool PF, class Load, class Store>
+__device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int Ns, bool inv, bool first, bool last,
+                                          const float2* __restrict__ tw, const float2* src, float2* dst,
+                                          Load& load, Store& store)
+{
+    const int nr = n / R;
+    const int total = P * nr;
+    const int twstride = n / (Ns * R);
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int p, j;
+        if (PF) { p = t % P; j = t / P; }
+        else    { j = t % nr; p = t / nr; }
+        const int jm = j % Ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int idx = j + r * nr;
+            v[r] = first ? load(p, idx) : src[p * ps + idx * is];
+        }
+        if (jm) {
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const float2 w = tw[jm * r * twstride];
+                v[r] = inv ? cmulc(v[r], w) : cmul(v[r], w);
+            }
+        }
+        Dft<R>::run(v, inv);
+        const int base = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int idx = base + r * Ns;
+            if (last) store(p, idx, v[r]);
+            else dst[p * ps + idx * is] = v[r];
+        }
+    }
+}
+
+// Run a full transform of P pencils.  Stage 0 reads through `load`, writes
+// bufA; stage s writes buf[s&1] (bufA, bufB alternating); the last stage
+// writes through `store`.  Ends with __syncthreads().  Requires nst >= 2.
+// Shared buffers must not alias anything `load` reads after stage 0.
+template <bool PF, class Load, class Store>
+__device__ void fft_run(const FftPlan& pl, const float2* __restrict__ tw, float2* bufA, float2* bufB,
+                        int P, int ps, int is, bool inv, Load load, Store store)
+{
+    int Ns = 1;
+    for (int s = 0; s < pl.nst; ++s) {
+        const bool first = (s == 0), last = (s == pl.nst - 1);
+        const float2* src = first ? nullptr : (((s - 1) & 1) ? bufB : bufA);
+        float2* dst = (s & 1) ? bufB : bufA;
+        switch (pl.rad[s]) {
+            case 2: fft_stage<2, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 3: fft_stage<3, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 4: fft_stage<4, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 5: fft_stage<5, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 7: fft_stage<7, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            default: fft_stage<8, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+        }
+        __syncthreads();
+        Ns *= pl.rad[s];
+    }
+}
+
+// Buffer that holds the output of fft_run when its store writes "the other"
+// buffer of the pair (the one the last stage does not read).
+__device__ __forceinline__ float2* fft_out_buf(const FftPlan& pl, float2* bufA, float2* bufB)
+{
+    return ((pl.nst - 1) & 1) ? bufB : bufA;
+}
+
+// Two real pencils a, b packed as z = a + i b and transformed together; this
+// recovers A(k) and B(k) from Z(k) and Zc = conj(Z(n-k)).
+__device__ __forceinline__ float2 unpack_a(float2 z, float2 zmc) { return make_float2(0.5f * (z.x + zmc.x), 0.5f * (z.y + zmc.y)); }
+__device__ __forceinline__ float2 unpack_b(float2 z, float2 zmc)
+{
+    // (z - zmc) / (2i)
+    return make_float2(0.5f * (z.y - zmc.y), -0.5f * (z.x - zmc.x));
+}
+
+// For z = a + i b transformed, the spectrum of M1 a + i M2 b (M1, M2
+// Hermitian multipliers) is 1/2 [(M1+M2) Z(k) + (M1-M2) conj(Z(n-k))].
+__device__ __forceinline__ float2 two_multiplier(float2 z, float2 zmc, float2 m1, float2 m2)
+{
+    float2 sp = cadd(m1, m2), sm = csub(m1, m2);
+    float2 r = cadd(cmul(sp, z), cmul(sm, zmc));
+    return cscale(r, 0.5f);
+}
+
+}  // namespace qvti

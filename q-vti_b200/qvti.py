@@ -1,0 +1,235 @@
+"""Python binding of libqvti.so (ctypes over the C ABI in include/qvti.h).
+
+The engine is the CUDA library; this module only marshals host arrays.  It
+mirrors the reference's operator surface for the path: a shot is the call of
+``cuda_forward_acoustic_3D`` (cuviscoelas_3D.cu:1137-1652) with the model,
+wavelet, source and receivers of viscoelas_3D.cpp, returning the three
+seismograms ``[it][ir]``.  There is no CPU fallback: loading fails loudly when
+the library is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqvti.so")
+
+SRC_FORCE_X = 0
+SRC_EXPLOSIVE = 1
+FIELDS = ("vx", "vy", "vz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz")
+
+
+class QvtiError(RuntimeError):
+    pass
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("ntx", ctypes.c_int), ("nty", ctypes.c_int), ("ntz", ctypes.c_int), ("pml", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("vti", ctypes.c_int),
+                ("device", ctypes.c_int), ("w0", ctypes.c_float)]
+
+
+_lib = None
+_F = ctypes.POINTER(ctypes.c_float)
+_I = ctypes.POINTER(ctypes.c_int)
+_D = ctypes.POINTER(ctypes.c_double)
+_V = ctypes.c_void_p
+
+
+def lib():
+    """Load libqvti.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QvtiError("libqvti.so not found at %s: build it with `make -C q-vti_b200`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        sig = {
+            "qvti_footprint_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
+            "qvti_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(_V)]),
+            "qvti_destroy": (ctypes.c_int, [_V]),
+            "qvti_set_model": (ctypes.c_int, [_V, _F, _F, _F, _F, _F, _F, _F, ctypes.c_int]),
+            "qvti_set_source": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F,
+                                               ctypes.c_int]),
+            "qvti_set_receivers": (ctypes.c_int, [_V, ctypes.c_int, _I, _I, ctypes.c_int]),
+            "qvti_reset": (ctypes.c_int, [_V]),
+            "qvti_step": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_step_timed": (ctypes.c_int, [_V, ctypes.c_int, _F]),
+            "qvti_sync": (ctypes.c_int, [_V]),
+            "qvti_steps_done": (ctypes.c_int, [_V]),
+            "qvti_get_records": (ctypes.c_int, [_V, _F, _F, _F]),
+            "qvti_get_fields": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _F]),
+            "qvti_device_field": (ctypes.c_int, [_V, ctypes.c_int, ctypes.POINTER(_F)]),
+            "qvti_field_norms": (ctypes.c_int, [_V, _D, _I]),
+            "qvti_forward_shot": (ctypes.c_int, [_V, _F, _F, _F, _F, _F, _F, _F, ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int, _I,
+                                                 _I, ctypes.c_int, _F, _F, _F]),
+            "qvti_derivative_1d": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _F, _F]),
+            "qvti_last_error": (ctypes.c_int, []),
+            "qvti_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise QvtiError("%s failed: %s (%d)" % (what, lib().qvti_error_string(rc).decode(), rc))
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(_F)
+
+
+def _f32(a, shape=None):
+    a = np.asarray(a, np.float32)
+    if shape is not None and a.ndim == 0:
+        a = np.full(shape, a, np.float32)
+    return np.ascontiguousarray(a)
+
+
+def footprint_bytes(ntx, nty, ntz, vti=False):
+    return int(lib().qvti_footprint_bytes(ntx, nty, ntz, 1 if vti else 0))
+
+
+class Simulation:
+    """One shot on one GPU: grid, model, source, receivers, wavefield state."""
+
+    def __init__(self, ntx, nty, ntz, pml, dx, dy, dz, dt, f0, vti=False, device=0, w0=0.0):
+        self.shape = (int(ntx), int(nty), int(ntz))
+        self.vti = bool(vti)
+        cfg = Config(int(ntx), int(nty), int(ntz), int(pml), float(dx), float(dy), float(dz), float(dt), float(f0),
+                     1 if vti else 0, int(device), float(w0))
+        h = _V()
+        _check(lib().qvti_create(ctypes.byref(cfg), ctypes.byref(h)), "qvti_create")
+        self._h = h
+        self.rn = 0
+        self.nt = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qvti_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_model(self, velp, vels, rho, gama_p, gama_s, eps=None, delta=None):
+        sh = self.shape
+        arrs = [_f32(a, sh) for a in (velp, vels, rho, gama_p, gama_s)]
+        e = _f32(eps, sh) if self.vti else None
+        d = _f32(delta, sh) if self.vti else None
+        for a in arrs:
+            if a.shape != sh:
+                raise QvtiError("model array shape %s != grid %s" % (a.shape, sh))
+        _check(lib().qvti_set_model(self._h, *[_fp(a) for a in arrs], _fp(e), _fp(d), 0), "qvti_set_model")
+
+    def set_model_device(self, ptrs):
+        """ptrs: device addresses (ints) of velp, vels, rho, gama_p, gama_s[, eps, delta]."""
+        p = [ctypes.cast(ctypes.c_void_p(int(x)), _F) for x in ptrs] + [None] * (7 - len(ptrs))
+        _check(lib().qvti_set_model(self._h, *p, 1), "qvti_set_model")
+
+    def set_source(self, s_ix, s_iy, s_iz, wavelet, kind=SRC_FORCE_X):
+        w = _f32(wavelet)
+        self.nt = w.size
+        _check(lib().qvti_set_source(self._h, int(kind), int(s_ix), int(s_iy), int(s_iz), _fp(w), w.size),
+               "qvti_set_source")
+
+    def set_receivers(self, r_iz, r_ix, r_iy):
+        rx = np.ascontiguousarray(r_ix, np.int32)
+        ry = np.ascontiguousarray(r_iy, np.int32)
+        self.rn = rx.size
+        _check(lib().qvti_set_receivers(self._h, int(r_iz), rx.ctypes.data_as(_I), ry.ctypes.data_as(_I), rx.size),
+               "qvti_set_receivers")
+
+    def reset(self):
+        _check(lib().qvti_reset(self._h), "qvti_reset")
+
+    def step(self, n=1):
+        _check(lib().qvti_step(self._h, int(n)), "qvti_step")
+
+    def step_timed(self, n):
+        ms = ctypes.c_float(0)
+        _check(lib().qvti_step_timed(self._h, int(n), ctypes.byref(ms)), "qvti_step_timed")
+        return ms.value
+
+    def sync(self):
+        _check(lib().qvti_sync(self._h), "qvti_sync")
+
+    @property
+    def steps_done(self):
+        return lib().qvti_steps_done(self._h)
+
+    def records(self):
+        n = self.steps_done
+        out = np.zeros((3, n, self.rn), np.float32)
+        _check(lib().qvti_get_records(self._h, _fp(out[0]), _fp(out[1]), _fp(out[2])), "qvti_get_records")
+        return out
+
+    def fields(self, first=0, count=9):
+        out = np.zeros((count,) + self.shape, np.float32)
+        _check(lib().qvti_get_fields(self._h, int(first), int(count), _fp(out)), "qvti_get_fields")
+        return out
+
+    def device_field(self, which):
+        p = _F()
+        _check(lib().qvti_device_field(self._h, int(which), ctypes.byref(p)), "qvti_device_field")
+        return ctypes.cast(p, ctypes.c_void_p).value
+
+    def norms(self):
+        out = np.zeros(9)
+        bad = ctypes.c_int(0)
+        rc = lib().qvti_field_norms(self._h, out.ctypes.data_as(_D), ctypes.byref(bad))
+        return out, bool(bad.value), rc
+
+    def derivative_1d(self, field, axis, forward):
+        f = _f32(field)
+        out = np.zeros_like(f)
+        _check(lib().qvti_derivative_1d(self._h, int(axis), 1 if forward else 0, _fp(f), _fp(out)),
+               "qvti_derivative_1d")
+        return out
+
+
+def simulation_for_case(c, vti=False, device=0):
+    return Simulation(c["ntx"], c["nty"], c["ntz"], c["pml"], c["dx"], c["dy"], c["dz"], c["dt"], c["f0"],
+                      vti=vti, device=device)
+
+
+def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=True, device=0, want_state=False):
+    """Run a shot described by a case dict (tests/qvti_cases.py conventions).
+
+    Returns dict(rec=[3, nt, rn], snaps={k: [3, ...]}, state=[9, ...] or None).
+    ``ref_offset`` adds the reference's +10 to s_iz (cuviscoelas_3D.cu:772)."""
+    nt = int(c["nt"] if nt is None else nt)
+    snaps = sorted(int(s) for s in snaps)
+    with simulation_for_case(c, vti=vti, device=device) as sim:
+        sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"],
+                      c.get("eps") if vti else None, c.get("delta") if vti else None)
+        sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])
+        sim.set_source(c["s_ix"], c["s_iy"], int(c["s_iz"]) + (10 if ref_offset else 0),
+                       np.asarray(c["rik"], np.float32)[:nt], kind=src_type)
+        sim.reset()
+        out = {}
+        done = 0
+        for k in snaps:
+            sim.step(k - done)
+            done = k
+            out[k] = sim.fields(0, 3)
+        sim.step(nt - done)
+        rec = sim.records()
+        state = sim.fields(0, 9) if want_state else None
+    return dict(rec=rec, snaps=out, state=state)

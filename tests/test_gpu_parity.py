@@ -1,0 +1,96 @@
+"""Parity of the CUDA path against the FP64 oracle and the reference's own
+cuFFT build (golden fixtures), through the C ABI.
+
+Tolerance: relative L2 <= 1e-4 on every seismogram component and every
+snapshot field at the end of the run (FP32 against FP64 and against the
+reference's FP32 cuFFT result).
+"""
+import numpy as np
+import pytest
+
+import qvti_cases as qc
+from conftest import golden_names, load_golden, snap_keys
+
+TOL = 1e-4
+pytestmark = pytest.mark.gpu
+
+
+def _compare(ours, ref, label):
+    worst = 0.0
+    for i, comp in enumerate(("vx", "vy", "vz")):
+        e = qc.relL2(ours["rec"][i], ref["rec"][i])
+        worst = max(worst, e)
+        assert e <= TOL, "%s seismogram %s relL2 %.3g" % (label, comp, e)
+    for k in ref.get("snaps", {}):
+        for i in range(3):
+            e = qc.relL2(ours["snaps"][k][i], ref["snaps"][k][i])
+            worst = max(worst, e)
+            assert e <= TOL, "%s snapshot %d field %d relL2 %.3g" % (label, k, i, e)
+    return worst
+
+
+@pytest.mark.parametrize("name", [n for n in golden_names() if n != "config1"])
+def test_against_reference_golden(qvti, name):
+    c = load_golden(name)
+    snaps = snap_keys(c)
+    ours = qvti.run_case(c, snaps=snaps, want_state=True)
+    ref = dict(rec=np.stack([c["rec_vx"], c["rec_vy"], c["rec_vz"]]),
+               snaps={k: c["snap_%d" % k] for k in snaps})
+    _compare(ours, ref, name)
+    for f in range(9):
+        e = qc.relL2(ours["state"][f], c["final9"][f])
+        assert e <= TOL, "%s final field %d relL2 %.3g" % (name, f, e)
+
+
+def test_config1_against_reference_golden(qvti):
+    """96^3, 20-cell C-PML, 500 steps: seismograms and final-state norms."""
+    c = load_golden("config1")
+    ours = qvti.run_case(c, want_state=True)
+    ref = dict(rec=np.stack([c["rec_vx"], c["rec_vy"], c["rec_vz"]]))
+    _compare(ours, ref, "config1")
+    norms = np.array([np.linalg.norm(f.astype(np.float64)) for f in ours["state"]])
+    rel = np.abs(norms - c["final_norms"]) / c["final_norms"]
+    assert rel.max() <= TOL, rel
+
+
+@pytest.mark.parametrize("name", [n for n in golden_names() if n != "config1"])
+def test_against_oracle(qvti, oracle, name):
+    c = load_golden(name)
+    snaps = snap_keys(c)
+    ours = qvti.run_case(c, snaps=snaps)
+    ref = oracle.run_case(c, snaps=snaps)
+    _compare(ours, ref, name)
+
+
+def _vti_case(seed=3):
+    c = qc.heterogeneous_case(n=(32, 32, 48), pml=8, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=90, f0=30.0,
+                              seed=seed, src=(16, 16, 20), r_iz=10, name="vti")
+    rng = np.random.default_rng(seed + 100)
+    shape = c["velp"].shape
+    c["eps"] = (0.05 + 0.2 * rng.random(shape)).astype(np.float32)
+    c["delta"] = (0.12 * rng.random(shape)).astype(np.float32)
+    return c
+
+
+def test_vti_against_oracle(qvti, oracle):
+    c = _vti_case()
+    ours = qvti.run_case(c, snaps=[45], vti=True)
+    ref = oracle.run_case(c, snaps=[45], vti=True)
+    _compare(ours, ref, "vti")
+
+
+def test_vti_zero_anisotropy_matches_isotropic(qvti):
+    c = _vti_case(seed=5)
+    c["eps"][:] = 0
+    c["delta"][:] = 0
+    a = qvti.run_case(c, vti=True)
+    b = qvti.run_case(c, vti=False)
+    for i in range(3):
+        assert qc.relL2(a["rec"][i], b["rec"][i]) <= 1e-6
+
+
+def test_explosive_source_against_oracle(qvti, oracle):
+    c = qc.heterogeneous_case(n=(32, 48, 32), pml=6, seed=11, src=(16, 24, 16), r_iz=8, nt=80, name="expl")
+    ours = qvti.run_case(c, snaps=[40], src_type=qvti.SRC_EXPLOSIVE, ref_offset=False)
+    ref = oracle.run_case(c, snaps=[40], src_type=1, ref_offset=False)
+    _compare(ours, ref, "explosive")
