@@ -1,0 +1,387 @@
+"""Benchmark: Gcell-steps/s of the 3D viscoelastic pseudospectral time step on
+the 256^3 VTI workload, one shot per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one time step of the whole padded 256^3 grid (PML inside); value =
+cells x steps x ranks / max-over-ranks device time of the K timed steps
+(CUDA events on the engine's stream).  Shots are independent, so N GPUs run
+N replicas of the shot with no data-path collective ("scaling": "weak");
+torch.distributed only provides the barrier and the max over ranks.
+
+``--impl reference`` times the reference's CPU counterpart: the reference has
+no CPU implementation of the path (it is CUDA + cuFFT), so the arm runs the
+FP64 CPU restatement (oracle/) on all host cores, each step a bounded sample
+(one time step of a centred crop of the same model, crop sized so the whole
+run ends in a few minutes), on rank 0 only.
+"""
+import argparse
+import contextlib
+import ctypes
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "q-vti_b200")
+
+GRID = (256, 256, 256)
+PML = 30  # C-PML cells per face (the 256^3 workload)
+DX = 10.0
+F0 = 20.0
+DT_NOMINAL = 0.8e-3
+SEED = 2024
+METRIC = "Gcell-steps/s 256^3 VTI"
+UNIT = "Gcell-steps/s"
+
+
+def _load(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Dist:
+    """Barrier and max-reduce over ranks: torch.distributed over NCCL on GPUs
+    (gloo when no GPU is visible, e.g. the CPU tests of this logic).  Shots
+    are independent, so this is the only cross-rank traffic."""
+
+    def __init__(self, world, local, backend=None):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            if backend is None:
+                backend = "nccl" if torch.cuda.is_available() else "gloo"
+            self.device = None
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+                self.device = torch.device("cuda", local)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.td, self.torch, self.local = td, torch, local
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            if self.device is not None:
+                self.td.barrier(device_ids=[self.local])
+            else:
+                self.td.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        t = self.torch.tensor([float(x)], dtype=self.torch.float64, device=self.device)
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.td.destroy_process_group()
+
+
+def aggregate_value(cells, steps, world, ms_max):
+    """Whole-job Gcell-steps/s: every rank advances its own shot `steps` steps."""
+    return cells * steps * world / (ms_max / 1e3) / 1e9
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9 and p[1].replace(".", "").isdigit():
+                    rows.append(p)
+        except OSError:
+            pass
+        finally:
+            with contextlib.suppress(OSError):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """dram read+write bytes per launch of `kernel` from the committed ncu
+    summaries (a line `traffic_bytes_per_launch <kernel> <bytes>`), or None."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            p = line.strip().strip("`").split()
+            if len(p) == 3 and p[0] == "traffic_bytes_per_launch" and p[1] == kernel:
+                return float(p[2])
+    return None
+
+
+def make_model(models):
+    m = models.layered_vti(tuple(GRID), DX, seed=SEED)
+    dt, lim, veff = models.choose_dt(m, DX, F0, DT_NOMINAL, vti=True)
+    return m, dt, lim, veff
+
+
+def workload_desc(dt):
+    return ("256^3 VTI: 6 layers Vp 1800-4500 m/s, Vs=Vp/1.8, Gardner rho, eps U[0.05,0.25], delta U[0,0.12], "
+            "Qp U[30,200], Qs=Qp/2, 5%% Gaussian perturbations (80 m), pml 30, dx 10 m, dt %.2f ms "
+            "(0.8 ms capped to 80%% of the CFL bound), 20 Hz Ricker force at (128,128,35), "
+            "256x256 receivers at iz=30, seed %d" % (dt * 1e3, SEED))
+
+
+# ----------------------------------------------------------------- CPU leg --
+def oracle_rate(model, crop, steps, warmup, dt, nthreads):
+    """Gcell-steps/s of the FP64 oracle on a centred crop^3 of the model."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    c0 = [(g - crop) // 2 for g in GRID]
+    sl = tuple(slice(a, a + crop) for a in c0)
+    pml = max(4, min(PML, crop // 6))
+    case = dict(ntx=crop, nty=crop, ntz=crop, pml=pml, nt=steps + warmup, dx=DX, dy=DX, dz=DX, dt=dt, f0=F0,
+                s_ix=crop // 2, s_iy=crop // 2, s_iz=pml + 5, r_iz=pml, r_ix=np.arange(crop, dtype=np.int32),
+                r_iy=np.full(crop, crop // 2, np.int32), rnx_max=crop, rny_max=1)
+    for k in ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta"):
+        case[k] = np.ascontiguousarray(model[k][sl])
+    models = _load("qvti_models", os.path.join(PKG, "models.py"))
+    case["rik"] = models.ricker(steps + warmup, dt, F0)
+    t0 = time.perf_counter()
+    orc.run_case(case, nt=max(warmup, 1), vti=True, ref_offset=False, nthreads=nthreads)
+    t1 = time.perf_counter()
+    orc.run_case(case, nt=max(warmup, 1) + steps, vti=True, ref_offset=False, nthreads=nthreads)
+    t2 = time.perf_counter()
+    sec = (t2 - t1) - (t1 - t0)  # the extra `steps` steps, setup cancelled
+    sec = max(sec, 1e-9)
+    return crop ** 3 * steps / sec / 1e9, sec
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    models = _load("qvti_models", os.path.join(PKG, "models.py"))
+    model, dt, _, _ = make_model(models)
+    cores = os.cpu_count() or 1
+    # size the crop so that warmup + steps oracle steps take ~150 s
+    probe_rate, _ = oracle_rate(model, 32, 2, 1, dt, cores)
+    budget = 150.0 / max(args.steps + args.warmup, 1)
+    crop = int((probe_rate * 1e9 * budget) ** (1 / 3) * 0.7)
+    crop = max(32, min(192, crop // 16 * 16))
+    rate, sec = oracle_rate(model, crop, args.steps, args.warmup, dt, cores)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": workload_desc(dt), "sample": "%d^3 crop" % crop},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": "FP64 CPU restatement (oracle/), %d timed steps of a centred %d^3 crop of the "
+                                   "same model, %d threads" % (args.steps, crop, cores)},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------- our arm --
+def our_arm(args, world, rank, local):
+    qv = _load("qvti_b200", os.path.join(PKG, "qvti.py"))
+    models = _load("qvti_models", os.path.join(PKG, "models.py"))
+    dist = Dist(world, local)
+    model, dt, lim, veff = make_model(models)
+    nx, ny, nz = GRID
+    ntp = nx * ny * nz
+    K, W = args.steps, args.warmup
+    nprof = 3
+    nt = W + K + nprof
+    rik = models.ricker(nt, dt, F0)
+    r_ix, r_iy = models.surface_receivers(nx, ny)
+    src = (nx // 2, ny // 2, PML + 5)
+
+    sim = qv.Simulation(nx, ny, nz, PML, DX, DX, DX, dt, F0, vti=True, device=local)
+    sim.set_model(model["velp"], model["vels"], model["rho"], model["gama_p"], model["gama_s"],
+                  model["eps"], model["delta"])
+    sim.set_receivers(PML, r_ix, r_iy)
+    sim.set_source(*src, rik, kind=qv.SRC_FORCE_X)
+    sim.reset()
+    sim.step(W)
+    sim.sync()
+
+    dist.barrier()
+    with ClockSampler(local) as clk:
+        ms = sim.step_timed(K)  # CUDA events on the engine's stream, synchronised
+    dist.barrier()
+    ms_max = dist.max(ms)
+    value = aggregate_value(ntp, K, world, ms_max)
+    clocks = clk.summary()
+
+    kernels = sim.profile_step(nprof)
+    norms, nonfinite, _ = sim.norms()
+    sim.close()
+
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "grid": list(GRID),
+                              "kernels": kernels, "finite": not nonfinite}), flush=True)
+        dist.close()
+        return 0
+    # end to end through the public C ABI: host model (pinned), host wavelet,
+    # receivers, K steps, seismograms back to host -- one call
+    import torch
+    pinned = {k: torch.from_numpy(model[k]).pin_memory() for k in
+              ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta")}
+    recs = torch.empty((3, K, nx * ny), dtype=torch.float32).pin_memory()
+    e2e_sim = qv.Simulation(nx, ny, nz, PML, DX, DX, DX, dt, F0, vti=True, device=local)
+    F = ctypes.POINTER(ctypes.c_float)
+    I = ctypes.POINTER(ctypes.c_int)
+
+    def fp(t):
+        return ctypes.cast(ctypes.c_void_p(t.data_ptr()), F)
+
+    rik_k = np.ascontiguousarray(rik[:K])
+    dist.barrier()
+    t0 = time.perf_counter()
+    rc = qv.lib().qvti_forward_shot(e2e_sim._h, *[fp(pinned[k]) for k in ("velp", "vels", "rho", "gama_p",
+                                                                            "gama_s", "eps", "delta")],
+                                    qv.SRC_FORCE_X, src[0], src[1], src[2], rik_k.ctypes.data_as(F), K, PML,
+                                    r_ix.ctypes.data_as(I), r_iy.ctypes.data_as(I), nx * ny,
+                                    fp(recs[0]), fp(recs[1]), fp(recs[2]))
+    t_e2e = time.perf_counter() - t0
+    e2e_sim.close()
+    if rc != 0:
+        raise SystemExit("qvti_forward_shot failed: %d" % rc)
+    t_e2e = dist.max(t_e2e)
+    e2e_value = ntp * K * world / t_e2e / 1e9
+    h2d = 7 * ntp * 4 + K * 4 + 2 * nx * ny * 4
+    d2h = 3 * K * nx * ny * 4
+
+    top = max(kernels, key=lambda k: k[1])
+    peak, peak_kind = measured_peaks()
+    achieved = top[2] / (top[1] / 1e3) / 1e9
+    traffic = ncu_traffic(top[0])
+    step_ms = sum(k[1] for k in kernels)
+    alg_bytes = sum(k[2] for k in kernels)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        rate, sec = oracle_rate(model, 96, 6, 1, dt, cores)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "FP64 CPU restatement (oracle/) on a centred 96^3 crop of the same model, 6 timed "
+                         "steps (%.1f s), %d threads" % (sec, cores)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_desc(dt), "grid": list(GRID), "pml": PML, "dt_s": dt,
+                       "cfl_dt_limit_s": lim, "form": "plain FP32",
+                       "l2": "inputs larger than L2 (~14 GB of fields and spectra per step)",
+                       "parallelism": "shot replicas, one per GPU" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "alg_bytes_per_launch": top[2], "ms_per_launch": top[1]},
+            "step_roofline": {"alg_bytes_per_cell_step": alg_bytes / ntp, "achieved_gbs": alg_bytes / (step_ms / 1e3) / 1e9,
+                              "canonical_B_alg_T63": 1177},
+            "kernels": [{"name": n, "ms": round(m, 4), "gbs": round(b / (m / 1e3) / 1e9, 1)} for n, m, b in kernels],
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+                    "seconds": t_e2e},
+            "gpu_launches": len(kernels) * K,
+            "clocks": clocks,
+            "finite": not nonfinite,
+        }
+        print(json.dumps(line), flush=True)
+    dist.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--grid", type=int, default=256, help="cube edge (profiling of smaller cases)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local = dist_setup()
+    if args.grid != 256:
+        global GRID, PML
+        GRID = (args.grid,) * 3
+        PML = min(30, max(4, args.grid // 8))
+    if args.impl == "reference":
+        return reference_arm(args, world, rank)
+    return our_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -129,6 +129,21 @@ int qvti_forward_shot(qvti_sim* sim, const float* velp, const float* vels, const
  * transforms it feeds).  For tests and diagnostics. */
 int qvti_derivative_1d(qvti_sim* sim, int axis, int fwd, const float* in, float* out);
 
+/* One constant-Q derivative field of a host field: out = Re IFFT3(|k|^power
+ * T(k_axis) FFT3(in)) / ntp, power in {-1, 0, 1} (the reference's Ap1, Ap2,
+ * Ap3, cuviscoelas_3D.cu:188-190) and T the forward (fwd=1) or backward
+ * staggered shift along `axis` -- one of the 45 fields of
+ * cuviscoelas_3D.cu:1342-1562 on its own.  For tests and diagnostics. */
+int qvti_q_derivative(qvti_sim* sim, int axis, int fwd, int power, const float* in, float* out);
+
+/* Per-kernel device time of the time step: runs nrep steps (advancing the
+ * state) with CUDA events between their kernels; sets *nkernels to the
+ * kernels per step and fills names (maxk*32 chars), the average ms per launch
+ * and each kernel's algorithmic HBM bytes per launch (maxk >= *nkernels).
+ * No counterpart in the reference, whose only timing is the CPU clock()
+ * around the whole program (viscoelas_3D.cpp:70-74, 472-480). */
+int qvti_profile_step(qvti_sim* sim, int nrep, int maxk, int* nkernels, char* names, float* ms, double* bytes);
+
 /* Last error code of this process and its description. */
 int qvti_last_error(void);
 const char* qvti_error_string(int code);

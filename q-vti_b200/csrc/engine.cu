@@ -2,6 +2,7 @@
 // replay of the step, and the qvti_* C ABI (include/qvti.h).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -42,18 +43,25 @@ bool smooth(int n)
     return n == 1;
 }
 
-// Radix schedule: radix 8 first, then 4, 2, and the odd radices.
+// Radix schedule: radix 16 first, then 8, 4, 2 and the odd radices (256 is
+// two radix-16 stages: one shared-memory exchange per transform).
 bool make_plan(int n, FftPlan* p)
 {
     p->n = n;
     p->nst = 0;
     int m = n;
+    while (m % 16 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 16; m /= 16; }
     while (m % 8 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 8; m /= 8; }
     while (m % 4 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 4; m /= 4; }
     while (m % 2 == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = 2; m /= 2; }
     for (int r : {3, 5, 7})
         while (m % r == 0 && p->nst < kMaxStages) { p->rad[p->nst++] = r; m /= r; }
     if (m != 1) return false;
+    if (p->nst == 1 && p->rad[0] == 16) {  // n = 16: two radix-4 stages
+        p->rad[0] = 4;
+        p->rad[1] = 4;
+        p->nst = 2;
+    }
     if (p->nst < 2) return false;
     return true;
 }
@@ -134,7 +142,7 @@ struct Sim {
     cudaStream_t st = nullptr;
     KP kp{};
     std::vector<void*> allocs;
-    float* coef[25] = {};
+    float* coef[12] = {};
     int* d_it = nullptr;
     float* d_rik = nullptr;
     int* d_rix = nullptr;
@@ -177,7 +185,7 @@ struct Sim {
 namespace {
 
 // Number of full-grid float arrays and half-spectrum complex arrays.
-constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 25 + 5 + 3;
+constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 12 + 5 + 3;
 constexpr int kSpecArrays = 3 + kNumG;
 
 int build_graph(Sim* s)
@@ -282,19 +290,29 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     float* rinv[3];
     for (int c = 0; c < 5; ++c) rc |= s->alloc(&mu[c], ntp);
     for (int c = 0; c < 3; ++c) rc |= s->alloc(&rinv[c], ntp);
-    for (int c = 0; c < 25; ++c) rc |= s->alloc(&s->coef[c], ntp);
+    for (int c = 0; c < 12; ++c) rc |= s->alloc(&s->coef[c], ntp);
     for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.H[c], nspec);
     for (int c = 0; c < kNumG; ++c) rc |= s->alloc(&k.G[c], nspec);
     rc |= s->alloc(&s->d_it, 1);
     rc |= s->alloc(&s->d_norm, 16);
     rc |= s->alloc(&s->d_bad, 4);
     if (rc) return bail(g_last_error);
-    for (int j = 0; j < 5; ++j) {
-        k.MU[j] = mu[j];
-        k.K11[j] = s->coef[j];
-        k.K12[j] = s->coef[5 + j];
-        k.K13[j] = s->coef[10 + j];
-        k.K33[j] = s->coef[15 + j];
+    for (int j = 0; j < 5; ++j) k.MU[j] = mu[j];
+    k.mrho = s->coef[0]; k.mgp = s->coef[1]; k.mgs = s->coef[2];
+    k.mc33 = s->coef[4]; k.mcs = s->coef[6];
+    // isotropic: c11 = c13 = c33, read from one array
+    k.mc11 = cfg->vti ? s->coef[3] : s->coef[4];
+    k.mc13 = cfg->vti ? s->coef[5] : s->coef[4];
+    k.w0 = cfg->w0 > 0 ? cfg->w0 : (float)(2 * 3.1415926 * cfg->f0);  // viscoelas_3D.cpp:109
+    // kz planes per batch of the k-space passes (k_cy fwd, k_mx, k_cy inv).
+    // Batches of ~48 MB of spectra would keep a batch in L2 between k_mx and
+    // the inverse y pass, but the small grids cost more than the saved HBM
+    // traffic (measured at 256^3), so the default is one batch;
+    // QVTI_KZ_BATCH overrides it for tuning.
+    {
+        int b = s->nkz;
+        if (const char* e = getenv("QVTI_KZ_BATCH")) b = atoi(e);
+        k.kz_batch = b < 1 ? 1 : (b > s->nkz ? s->nkz : b);
     }
     for (int c = 0; c < 3; ++c) k.rinv[c] = rinv[c];
     k.d_it = s->d_it;
@@ -338,12 +356,12 @@ extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels,
         }
     }
     float** d_coef = nullptr;
-    QV_CUDA(cudaMalloc(&d_coef, sizeof(float*) * 25));
-    QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 25, cudaMemcpyHostToDevice, s->st));
-    const float w0 = s->cfg.w0 > 0 ? s->cfg.w0 : (float)(2 * 3.1415926 * s->cfg.f0);  // viscoelas_3D.cpp:109
+    QV_CUDA(cudaMalloc(&d_coef, sizeof(float*) * 12));
+    QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 12, cudaMemcpyHostToDevice, s->st));
+    const float w0 = s->kp.w0;
     launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
                       s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, w0, d_coef, s->st);
-    launch_mu_rinv(s->kp, dev[2], s->coef + 20, s->st);
+    launch_mu_rinv(s->kp, dev[2], s->coef + 7, s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
     cudaFree(d_coef);
@@ -575,6 +593,98 @@ extern "C" int qvti_derivative_1d(qvti_sim* s, int axis, int fwd, const float* i
     QV_CUDA(cudaMalloc(&dout, b));
     QV_CUDA(cudaMemcpy(din, in, b, cudaMemcpyHostToDevice));
     launch_derivative_1d(s->kp, axis, fwd, din, dout, s->st);
+    QV_CUDA(cudaGetLastError());
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    QV_CUDA(cudaMemcpy(out, dout, b, cudaMemcpyDeviceToHost));
+    cudaFree(din);
+    cudaFree(dout);
+    return QVTI_OK;
+}
+
+// Algorithmic HBM bytes of each step kernel: the reads and writes its job
+// needs once each (full-grid fields, half spectra, C-PML variables in their
+// slabs only), no re-reads.
+static void kernel_bytes(const qvti_sim* s, double* b)
+{
+    const double F = 4.0 * s->ntp, S = 8.0 * s->nkz * (double)s->nx * s->ny;
+    const int pml = s->cfg.pml;
+    auto slab = [&](int n) { int c = 0; for (int i = 0; i < n - 1; ++i) c += (i < pml || i >= n - pml); return (double)c; };
+    const double gx = s->nx - 1, gy = s->ny - 1, gz = s->nz - 1;
+    const double cx = slab(s->nx) * gy * gz, cy = slab(s->ny) * gx * gz, cz = slab(s->nz) * gx * gy;
+    const double model = (s->cfg.vti ? 7 : 5) * F;
+    b[0] = 3 * F + 6 * F + 24 * cy;                                        // k_vy
+    b[1] = 3 * F + 6 * F + 3 * F + 3 * F + 24 * cx;                        // k_vx
+    b[2] = 3 * F + 3 * S;                                                  // k_fz
+    b[3] = 3 * 2 * S;                                                      // k_cy_fwd
+    b[4] = 3 * S + qvti::kNumG * S;                                        // k_mx
+    b[5] = qvti::kNumG * 2 * S;                                            // k_cy_inv
+    // k_sigma: 27 half spectra, 6 stresses and 6 loss potentials read+written,
+    // model + MU, 3 R written, C-PML variables in their slabs
+    b[6] = qvti::kNumG * S + 12 * F + 12 * F + model + 5 * F + 3 * F + 3 * 8 * cz +
+           (48 + 16 + 16) * cx + (48 + 16 + 16) * cy + (32 + 16 + 16) * cz;
+    b[7] = s->rn * (3 * 4.0 * 2 + 8.0);                                    // k_rec
+}
+
+// Per-kernel device time of the step (CUDA events between the kernels of
+// nrep consecutive steps on the simulation's stream; the steps advance the
+// state like qvti_step).  names: maxk*32 chars; ms, bytes: maxk each;
+// *nkernels receives the number of kernels per step.
+extern "C" int qvti_profile_step(qvti_sim* s, int nrep, int maxk, int* nkernels, char* names, float* ms,
+                                 double* bytes)
+{
+    using namespace qvti;
+    if (!s || nrep <= 0 || maxk < kStepKernels) return fail(QVTI_ERR_ARG);
+    if (!s->have_model || !s->have_src) return fail(QVTI_ERR_STATE);
+    if (s->steps + nrep > s->nt) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    StepProfile* prof = new StepProfile();
+    for (auto& e : prof->ev) QV_CUDA(cudaEventCreate(&e));
+    std::vector<double> acc(kStepKernels, 0.0);
+    int rc = QVTI_OK;
+    for (int r = 0; r < nrep && rc == QVTI_OK; ++r) {
+        prof->n = 0;
+        launch_step(s->kp, s->st, prof);
+        if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(prof->ev[prof->n - 1]) != cudaSuccess) {
+            rc = fail(QVTI_ERR_CUDA);
+            break;
+        }
+        for (int i = 1; i < prof->n; ++i) {
+            float t = 0;
+            cudaEventElapsedTime(&t, prof->ev[i - 1], prof->ev[i]);
+            if (prof->kind[i] >= 0 && prof->kind[i] < kStepKernels) acc[prof->kind[i]] += t;
+        }
+        s->steps += 1;
+    }
+    for (auto& e : prof->ev) cudaEventDestroy(e);
+    delete prof;
+    if (rc) return rc;
+    double b[kStepKernels];
+    kernel_bytes(s, b);
+    for (int i = 0; i < kStepKernels; ++i) {
+        if (names) { std::strncpy(names + 32 * i, kStepKernelNames[i], 31); names[32 * i + 31] = 0; }
+        if (ms) ms[i] = (float)(acc[i] / nrep);
+        if (bytes) bytes[i] = b[i];
+    }
+    if (nkernels) *nkernels = kStepKernels;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_q_derivative(qvti_sim* s, int axis, int fwd, int power, const float* in, float* out)
+{
+    using namespace qvti;
+    if (!s || !in || !out || axis < 0 || axis > 2 || power < -1 || power > 1) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    float *din = nullptr, *dout = nullptr;
+    const size_t b = sizeof(float) * s->ntp;
+    QV_CUDA(cudaMalloc(&din, b));
+    QV_CUDA(cudaMalloc(&dout, b));
+    QV_CUDA(cudaMemcpy(din, in, b, cudaMemcpyHostToDevice));
+    KP k = s->kp;
+    k.v[0] = din;
+    k.H[0] = s->kp.G[0];  // scratch: rewritten by every time step anyway
+    k.G[0] = s->kp.G[0];
+    launch_q_derivative(k, axis, fwd, power, dout, s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
     QV_CUDA(cudaMemcpy(out, dout, b, cudaMemcpyDeviceToHost));

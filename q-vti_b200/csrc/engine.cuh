@@ -15,7 +15,8 @@
 //   C-PML      memory variables and per-term loss potentials, allocated
 //              full size but read/written only inside their axis slab
 //              (they are identically zero elsewhere, b = 0 there)   float
-//   coef       K11 K12 K13 K33 (5 each: eta1 eta2 eta3 tau1 tau2), MU (5,
+//   coef       rho, gamma_p, gamma_s and the effective velocities of c11,
+//              c33, c13, c44 (7; 5 distinct when isotropic), MU (5, the
 //              8-point averaged shear set), 1/rho-bar per velocity component;
 //              built once per shot in FP64 and rounded              float
 //   H[3]       velocity spectra, half along z: [kz][x][y], nkz = nz/2+1 float2
@@ -53,11 +54,13 @@ struct KP {
     float* qn[8];    // matching per-term loss potentials
     float* phs[6];   // shear memory variables: vx_z vz_x vx_y vy_x vy_z vz_y
     float* qs[6];
-    // coefficients
-    const float* K11[5];
-    const float* K12[5];
-    const float* K13[5];
-    const float* K33[5];
+    // coefficients (built in FP64 at setup): density, constant-Q exponents and
+    // the effective velocities c = v cos(pi gamma / 2) of the moduli c11, c33,
+    // c13 (P-type, gamma_p) and c44 = c66 (S-type, gamma_s); the eta/tau sets
+    // are rebuilt from them on chip.  MU: 8-point averaged shear set; rinv:
+    // 1/rho-bar of vx, vy, vz.
+    const float *mrho, *mgp, *mgs, *mc11, *mc33, *mc13, *mcs;
+    float w0;
     const float* MU[5];
     const float* rinv[3];
     // spectra
@@ -70,10 +73,21 @@ struct KP {
     const int *r_ix, *r_iy;
     float* rec[3];
     int* d_it;       // current step index, advanced on the device each step
+    int kz_batch;    // kz planes per batch of the k-space passes
 };
 
 // Host-side launchers (step_kernels.cu).  All launch on `st`.
-void launch_step(const KP& kp, cudaStream_t st);
+constexpr int kStepKernels = 8;
+extern const char* const kStepKernelNames[kStepKernels];
+struct StepProfile {
+    static constexpr int kMax = 1024;
+    cudaEvent_t ev[kMax];
+    int kind[kMax];   // kernel index of the launch that ends at ev[i]; -1 = start
+    int n = 0;
+};
+void launch_step(const KP& kp, cudaStream_t st, StepProfile* prof = nullptr);
+// coef_out: 7 model arrays (rho gp gs c11 c33 c13 cs) then the 5 S-set arrays
+// (input of the MU average).
 void launch_coef_build(const KP& kp, const float* velp, const float* vels, const float* rho,
                        const float* gp, const float* gs, const float* eps, const float* delta, int vti,
                        float w0, float* const* coef_out, cudaStream_t st);
@@ -81,6 +95,7 @@ void launch_mu_rinv(const KP& kp, const float* rho, const float* const* sset, cu
 int configure_kernels();   // raise dynamic shared-memory limits, returns cudaError_t
 
 // Individual stages, exposed for unit tests through the C ABI.
+void launch_q_derivative(const KP& kp, int axis, int fwd, int pw, float* out, cudaStream_t st);
 void launch_derivative_1d(const KP& kp, int axis, int fwd_shift, const float* in, float* out, cudaStream_t st);
 
 }  // namespace qvti

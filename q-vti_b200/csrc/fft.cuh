@@ -3,7 +3,7 @@
 // The spectral-derivative engine replaces the reference's 63 cuFFT C2C calls
 // per step (cuviscoelas_3D.cu:1272-1562) with pencil kernels that transform a
 // tile of P pencils of one axis on chip.  A transform of length n = prod(rad)
-// runs as a Stockham autosort sequence of radix-2/3/4/5/7/8 stages:
+// runs as a Stockham autosort sequence of radix-2/3/4/5/7/8/16 stages:
 //
 //   * stage 0 reads its inputs through a caller-supplied `load(p, i)` functor
 //     (straight from global memory, or from shared memory with a k-space
@@ -162,10 +162,69 @@ struct Dft<5> : DftOdd<5> {};
 template <>
 struct Dft<7> : DftOdd<7> {};
 
+// Radix 16 in registers as 4 x 4: DFT-4 over n2 of v[n1 + 4 n2], twiddle
+// W16^{n1 k2}, DFT-4 over n1; output X[k2 + 4 k1].
+__device__ __forceinline__ float2 w16(float2 a, int e, bool inv)
+{
+    const float c1 = 0.923879533f, s1 = 0.382683432f, r = 0.707106781f;
+    float c, s;
+    switch (e & 15) {
+        case 0: c = 1.f; s = 0.f; break;
+        case 1: c = c1; s = s1; break;
+        case 2: c = r; s = r; break;
+        case 3: c = s1; s = c1; break;
+        case 4: c = 0.f; s = 1.f; break;
+        case 5: c = -s1; s = c1; break;
+        case 6: c = -r; s = r; break;
+        case 7: c = -c1; s = s1; break;
+        case 8: c = -1.f; s = 0.f; break;
+        case 9: c = -c1; s = -s1; break;
+        case 10: c = -r; s = -r; break;
+        case 11: c = -s1; s = -c1; break;
+        case 12: c = 0.f; s = -1.f; break;
+        case 13: c = s1; s = -c1; break;
+        case 14: c = r; s = -r; break;
+        default: c = c1; s = -s1; break;
+    }
+    // forward W16^e = cos - i sin, inverse its conjugate
+    if (!inv) s = -s;
+    return make_float2(a.x * c - a.y * s, a.x * s + a.y * c);
+}
+
+template <>
+struct Dft<16> {
+    static __device__ __forceinline__ void run(float2* v, bool inv)
+    {
+        float2 y[16];
+#pragma unroll
+        for (int n1 = 0; n1 < 4; ++n1) {
+            float2 t[4] = {v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]};
+            Dft<4>::run(t, inv);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2) y[n1 * 4 + k2] = (n1 && k2) ? w16(t[k2], n1 * k2, inv) : t[k2];
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) {
+            float2 t[4] = {y[k2], y[4 + k2], y[8 + k2], y[12 + k2]};
+            Dft<4>::run(t, inv);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; ++k1) v[k2 + 4 * k1] = t[k1];
+        }
+    }
+};
+
 // ------------------------------------------------------------------- stages
+// Shared-memory address of element (p, i): p*ps + i*is, plus one extra `is`
+// row every 2^padsh indices when padsh > 0 (breaks the bank conflicts of the
+// radix-16 stage-0 writes in pencil-fastest tiles).
+__device__ __forceinline__ int smem_at(int p, int i, int ps, int is, int padsh)
+{
+    return p * ps + i * is + (padsh ? (i >> padsh) * is : 0);
+}
+
 template <int R, bool PF, class Load, class Store>
-__device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int Ns, bool inv, bool first, bool last,
-                                          const float2* __restrict__ tw, const float2* src, float2* dst,
+__device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int padsh, int Ns, bool inv, bool first,
+                                          bool last, const float2* __restrict__ tw, const float2* src, float2* dst,
                                           Load& load, Store& store)
 {
     const int nr = n / R;
@@ -180,7 +239,7 @@ __device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int Ns, 
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const int idx = j + r * nr;
-            v[r] = first ? load(p, idx) : src[p * ps + idx * is];
+            v[r] = first ? load(p, idx) : src[smem_at(p, idx, ps, is, padsh)];
         }
         if (jm) {
 #pragma unroll
@@ -195,7 +254,7 @@ __device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int Ns, 
         for (int r = 0; r < R; ++r) {
             const int idx = base + r * Ns;
             if (last) store(p, idx, v[r]);
-            else dst[p * ps + idx * is] = v[r];
+            else dst[smem_at(p, idx, ps, is, padsh)] = v[r];
         }
     }
 }
@@ -206,7 +265,7 @@ __device__ __forceinline__ void fft_stage(int n, int P, int ps, int is, int Ns, 
 // Shared buffers must not alias anything `load` reads after stage 0.
 template <bool PF, class Load, class Store>
 __device__ void fft_run(const FftPlan& pl, const float2* __restrict__ tw, float2* bufA, float2* bufB,
-                        int P, int ps, int is, bool inv, Load load, Store store)
+                        int P, int ps, int is, bool inv, Load load, Store store, int padsh = 0)
 {
     int Ns = 1;
     for (int s = 0; s < pl.nst; ++s) {
@@ -214,12 +273,13 @@ __device__ void fft_run(const FftPlan& pl, const float2* __restrict__ tw, float2
         const float2* src = first ? nullptr : (((s - 1) & 1) ? bufB : bufA);
         float2* dst = (s & 1) ? bufB : bufA;
         switch (pl.rad[s]) {
-            case 2: fft_stage<2, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
-            case 3: fft_stage<3, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
-            case 4: fft_stage<4, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
-            case 5: fft_stage<5, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
-            case 7: fft_stage<7, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
-            default: fft_stage<8, PF>(pl.n, P, ps, is, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 2: fft_stage<2, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 3: fft_stage<3, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 4: fft_stage<4, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 5: fft_stage<5, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 7: fft_stage<7, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            case 16: fft_stage<16, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
+            default: fft_stage<8, PF>(pl.n, P, ps, is, padsh, Ns, inv, first, last, tw, src, dst, load, store); break;
         }
         __syncthreads();
         Ns *= pl.rad[s];

@@ -42,6 +42,12 @@ __device__ __forceinline__ long long spec(const KP& k, int kz, int x, int y)
 }
 __device__ __forceinline__ bool in_slab(int i, int n, int pml) { return i < pml || i >= n - pml; }
 
+// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2.
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ void load_table(float2* s, const float2* g, int n)
 {
     for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
@@ -88,29 +94,37 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P)
 }
 
 // ------------------------------------------------------------------ k_cy --
-// C2C along y, in place, on L contiguous y lines per block.  arr selects the
-// field (H[0..2] forward or G[0..26] inverse).
+// C2C along y, in place, on L contiguous y lines per block (lines (kz, x)
+// starting at line0).  Pencil-fastest mapping: a warp covers 32/L consecutive
+// points of each of its L lines, so each global access is a full 32-byte
+// sector per line (L = 8) and the shared-memory stages are conflict-free.
+// The field is H[0..2] (forward) or G[0..26] (inverse), by blockIdx.y.
+constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
+
 template <bool INV>
-__global__ void __launch_bounds__(kThreads) k_cy(KP k, int L)
+__global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L, long long line0)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.ny, ps = n + 1;
+    const int n = k.ny;
     float2* tw = sm;
     float2* A = tw + n;
-    float2* B = A + L * ps;
+    float2* B = A + L * (n + n / 16);
     load_table(tw, k.tw_y, n);
     __syncthreads();
     float2* arr = INV ? k.G[blockIdx.y] : k.H[blockIdx.y];
-    float2* base = arr + (long long)blockIdx.x * L * n;
+    float2* base = arr + (line0 + (long long)blockIdx.x * L) * n;
     auto load = [&](int p, int i) -> float2 { return base[(long long)p * n + i]; };
     auto store = [&](int p, int i, float2 v) { base[(long long)p * n + i] = v; };
-    fft_run<false>(k.py, tw, A, B, L, ps, 1, INV, load, store);
+    fft_run<true>(k.py, tw, A, B, L, 1, L, INV, load, store, 4);
 }
 
 // ------------------------------------------------------------------ k_mx --
-// x-pencils of the (kz, y-chunk) tile in k-space.
-__global__ void __launch_bounds__(kThreads) k_mx(KP k, int P)
+// x-pencils of a (kz, y-chunk) tile in k-space for one velocity component c
+// (blockIdx.z): forward x-FFT of V_c, then the 9 fields that use V_c --
+// 3 derivatives x 3 dispersion operators Ap_j D_d V_c -- each inverse
+// x-transformed on chip.  blockIdx.y + kz0 is the kz plane.
+__global__ void __launch_bounds__(kThreads) k_mx(KP k, int P, int kz0)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
@@ -118,224 +132,344 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P)
     float2* tw = sm;
     float2* tFx = tw + n;
     float2* tBx = tFx + n;
-    float2* V = tBx + n;            // [3][n][P]
-    float2* A = V + 3 * n * P;
-    float2* B = A + n * P;
-    float* tkx = reinterpret_cast<float*>(B + n * P);
+    float2* V = tBx + n;            // [n][P]
+    float2* A = V + n * P;
+    float2* B = A + (n + n / 16) * P;
+    float* tkx = reinterpret_cast<float*>(B + (n + n / 16) * P);
     load_table(tw, k.tw_x, n);
     load_table(tFx, k.Fx, n);
     load_table(tBx, k.Bx, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) tkx[i] = k.kx[i];
     __syncthreads();
-    const int kz = blockIdx.y, y0 = blockIdx.x * P;
+    const int kz = kz0 + blockIdx.y, y0 = blockIdx.x * P, c = blockIdx.z;
 
-    for (int f = 0; f < 3; ++f) {
-        const float2* H = k.H[f];
-        float2* Vf = V + f * n * P;
+    {
+        const float2* H = k.H[c];
         auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
-        auto store = [&](int p, int i, float2 v) { Vf[i * P + p] = v; };
-        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store);
+        auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
+        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store, 4);
     }
 
     const float kzv = k.kz[kz];
     const float kz2 = kzv * kzv;
     const float2 tFz = k.Fz[kz], tBz = k.Bz[kz];
-    for (int o = 0; o < kNumG; ++o) {
-        const int d = o / 3, j = o % 3;
-        const int c = c_comp[d], ax = c_axis[d], fw = c_fwd[d];
-        const float2* Vc = V + c * n * P;
-        float2* G = k.G[o];
-        auto load = [&](int p, int i) -> float2 {
-            const float kyv = k.ky[y0 + p];
-            const float kxv = tkx[i];
-            float k2 = kxv * kxv + kyv * kyv + kz2;
-            k2 = fmaxf(k2, 1e-10f);  // the reference sets |k|^2 = 1e-10 at DC (cu:74)
-            const float ap = j == 1 ? 1.0f : (j == 0 ? 1.0f / sqrtf(k2) : sqrtf(k2));
-            float2 T;
-            if (ax == 0) T = fw ? tFx[i] : tBx[i];
-            else if (ax == 1) T = fw ? k.Fy[y0 + p] : k.By[y0 + p];
-            else T = fw ? tFz : tBz;
-            return cmul(Vc[i * P + p], cscale(T, ap * k.inv_ntp));
-        };
-        auto store = [&](int p, int i, float2 v) { G[spec(k, kz, i, y0 + p)] = v; };
-        fft_run<true>(k.px, tw, A, B, P, 1, P, true, load, store);
+    for (int d = 0; d < 9; ++d) {
+        if (c_comp[d] != c) continue;
+        const int ax = c_axis[d], fw = c_fwd[d];
+        for (int j = 0; j < 3; ++j) {
+            float2* G = k.G[3 * d + j];
+            auto load = [&](int p, int i) -> float2 {
+                const float kyv = k.ky[y0 + p];
+                const float kxv = tkx[i];
+                float k2 = kxv * kxv + kyv * kyv + kz2;
+                k2 = fmaxf(k2, 1e-10f);  // the reference sets |k|^2 = 1e-10 at DC (cu:74)
+                const float ap = j == 1 ? 1.0f : (j == 0 ? 1.0f / sqrtf(k2) : sqrtf(k2));
+                float2 T;
+                if (ax == 0) T = fw ? tFx[i] : tBx[i];
+                else if (ax == 1) T = fw ? k.Fy[y0 + p] : k.By[y0 + p];
+                else T = fw ? tFz : tBz;
+                return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
+            };
+            auto store = [&](int p, int i, float2 v) { G[spec(k, kz, i, y0 + p)] = v; };
+            fft_run<true>(k.px, tw, A, B, P, 1, P, true, load, store, 4);
+        }
     }
 }
 
-// ------------------------------------------------------------------ k_iz --
-// z-pencils: C2R of the group's derivative fields, stress update, source
-// injection and the z derivative of the updated stress for the next velocity
-// update.  GRP 0: sxx syy szz (G 0..8), 1: sxz (G 9..14), 2: sxy (G 15..20),
-// 3: syz (G 21..26).
-template <int GRP>
-__global__ void __launch_bounds__(kThreads) k_iz(KP k, int P)
+// --------------------------------------------------------------- k_sigma --
+// Constant-Q set of one modulus from its effective velocity c = v cos(pi g/2)
+// (cuviscoelas_3D.cu:195-205): eta1 = -rho c g w0, eta2 = rho c^2,
+// eta3 = rho c^3 g / w0, tau1 = rho c g pi, tau2 = rho c^2 g^2 pi / w0.
+// c is built in FP64 at setup; the products are rebuilt here in FP32.
+__device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, float inv_w0, float o[5])
 {
-    constexpr int NF = GRP == 0 ? 9 : 6;
+    const float pi = 3.1415926f;
+    const float rc = rho * c, rc2 = rc * c;
+    o[0] = -rc * g * w0;
+    o[1] = rc2;
+    o[2] = rc2 * c * g * inv_w0;
+    o[3] = rc * g * pi;
+    o[4] = rc2 * g * g * pi * inv_w0;
+}
+
+// z-pencils of one x and P y rows (P/2 pencil pairs): C2R of the 27
+// derivative fields group by group (normal: G 0..8, xz: 9..14, xy: 15..20,
+// yz: 21..26), each group batched into one transform and followed by its
+// stress update; then the z derivatives of the new szz, sxz, syz for the next
+// velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
+// z terms, and the source injection.
+__global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
+{
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int n = k.nz, Qp = P / 2, np1 = n + 1, nx = k.nx, ny = k.ny, pml = k.pml;
+    const int two_buf = k.pz.nst > 2;
     float2* tw = sm;
     float2* A = tw + n;
-    float2* B = A + Qp * np1;
-    float* S = reinterpret_cast<float*>(B + Qp * np1);  // [NF][P][np1]
+    float2* B = A + 9 * Qp * n;  // aliases S when the transform has two stages
+    float* S = reinterpret_cast<float*>(B + (two_buf ? 9 * Qp * n : 0));  // [9][P][np1]
+    float* D = S + 9 * P * np1;                                           // [3][P][np1]: szz sxz syz
     load_table(tw, k.tw_z, n);
     __syncthreads();
     const int x = blockIdx.y, y0 = blockIdx.x * P;
-    const int o0 = GRP == 0 ? 0 : 9 + (GRP - 1) * 6;
     const int it = *k.d_it;
     const float dt = k.dt, inv_dt = 1.0f / k.dt;
+    const float w0 = k.w0, inv_w0 = 1.0f / k.w0;
+    const long long src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
 
-    // 1. C2R along z: pencils (2q, 2q+1) of the half spectra packed as A + iB.
-    for (int f = 0; f < NF; ++f) {
-        const float2* g = k.G[o0 + f];
-        float* Sf = S + f * P * np1;
-        auto load = [&](int q, int i) -> float2 {
+    // L2 prefetch of a group's inputs: the P-row slices of its half spectra
+    // (one 8P-byte run per kz) and the contiguous P*nz runs of the stresses,
+    // loss potentials and coefficients its update reads.  Issued one group
+    // ahead, so each phase's loads hit L2 instead of waiting on HBM.
+    auto prefetch_group = [&](int g) {
+        if (g > 3) return;
+        const int nf = g == 0 ? 9 : 6, of = g == 0 ? 0 : 9 + (g - 1) * 6;
+        const unsigned row = 8u * P;
+        for (int t = threadIdx.x; t < nf * k.nkz; t += blockDim.x) {
+            const int f = t / k.nkz, kz = t - f * k.nkz;
+            prefetch_l2(k.G[of + f] + spec(k, kz, x, y0), row);
+        }
+        const long long c0 = cell(k, x, y0, 0);
+        const unsigned run = 4u * P * n;
+        if (threadIdx.x == 0) {
+            if (g == 0) {
+                const float* arr[13] = {k.s[0], k.s[1], k.s[2], k.Q[0], k.Q[1], k.Q[2], k.mrho, k.mgp, k.mgs,
+                                        k.mc11, k.mc33, k.mc13, k.mcs};
+                for (int a = 0; a < 13; ++a) prefetch_l2(arr[a] + c0, run);
+            } else {
+                const int sidx = g == 1 ? 4 : g == 2 ? 3 : 5;
+                prefetch_l2(k.s[sidx] + c0, run);
+                prefetch_l2(k.Q[sidx] + c0, run);
+                for (int j = 0; j < 5; ++j) prefetch_l2(k.MU[j] + c0, run);
+            }
+        }
+    };
+    prefetch_group(0);
+
+    for (int grp = 0; grp < 4; ++grp) {
+        const int NF = grp == 0 ? 9 : 6;
+        const int o0 = grp == 0 ? 0 : 9 + (grp - 1) * 6;
+        const int npen = NF * Qp;
+        prefetch_group(grp + 1);
+        // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
+        //    of field f packed as A + iB (Hermitian extension of the half
+        //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
+        auto load = [&](int pp, int i) -> float2 {
+            const int f = pp / Qp, q = pp - f * Qp;
             const int kk = i <= n / 2 ? i : n - i;
-            const float4 gg = *reinterpret_cast<const float4*>(g + spec(k, kk, x, y0 + 2 * q));
+            const float4 gg = *reinterpret_cast<const float4*>(k.G[o0 + f] + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
             if (kk == 0 || 2 * kk == n) { a.y = 0.f; b.y = 0.f; }
             if (i > n / 2) { a.y = -a.y; b.y = -b.y; }
             return make_float2(a.x - b.y, a.y + b.x);
         };
-        auto store = [&](int q, int i, float2 v) {
-            Sf[(2 * q) * np1 + i] = v.x;
-            Sf[(2 * q + 1) * np1 + i] = v.y;
+        auto store = [&](int pp, int i, float2 v) {
+            const int f = pp / Qp, q = pp - f * Qp;
+            S[(f * P + 2 * q) * np1 + i] = v.x;
+            S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_run<true>(k.pz, tw, A, B, Qp, 1, Qp, true, load, store);
-    }
+        fft_run<true>(k.pz, tw, A, B, npen, 1, npen, true, load, store);
 
-    // 2. cell updates.  The updated stress that feeds the z derivative is
-    //    parked in S[0] (each cell's S values are read by its own thread only).
-    const long long src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
-    for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
-        const int p = t / n, z = t % n, y = y0 + p;
-        const long long ip = cell(k, x, y, z);
-        const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
-        auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
-        float out;
-        if constexpr (GRP == 0) {
-            float sxx = k.s[0][ip], syy = k.s[1][ip], szz = k.s[2][ip];
-            if (upd) {
-                float a11[5], a12[5], a13[5], a33[5];
+        // 2. stress update of the group.  Each thread owns kCells cells; all
+        //    their streaming inputs are loaded before any store so the loads
+        //    are in flight together (the arrays cannot alias, but the
+        //    compiler cannot know that through the parameter struct).
+        constexpr int kCells = 1;
+        for (int t0 = threadIdx.x; t0 < P * n; t0 += kCells * blockDim.x) {
+            if (grp == 0) {
+                float* __restrict__ s0 = k.s[0];
+                float* __restrict__ s1 = k.s[1];
+                float* __restrict__ s2 = k.s[2];
+                float* __restrict__ q0 = k.Q[0];
+                float* __restrict__ q1 = k.Q[1];
+                float* __restrict__ q2 = k.Q[2];
+                float in[kCells][13];
+                long long ipv[kCells];
+                bool ok[kCells];
 #pragma unroll
-                for (int j = 0; j < 5; ++j) {
-                    a11[j] = k.K11[j][ip]; a12[j] = k.K12[j][ip];
-                    a13[j] = k.K13[j][ip]; a33[j] = k.K33[j][ip];
+                for (int u = 0; u < kCells; ++u) {
+                    const int t = t0 + u * blockDim.x;
+                    ok[u] = t < P * n;
+                    const int p = t / n, z = t - p * n;
+                    ipv[u] = cell(k, x, y0 + p, z);
+                    if (ok[u]) {
+                        const long long ip = ipv[u];
+                        in[u][0] = s0[ip]; in[u][1] = s1[ip]; in[u][2] = s2[ip];
+                        in[u][3] = q0[ip]; in[u][4] = q1[ip]; in[u][5] = q2[ip];
+                        in[u][6] = __ldg(k.mrho + ip); in[u][7] = __ldg(k.mgp + ip); in[u][8] = __ldg(k.mgs + ip);
+                        in[u][9] = __ldg(k.mc11 + ip); in[u][10] = __ldg(k.mc33 + ip);
+                        in[u][11] = __ldg(k.mc13 + ip); in[u][12] = __ldg(k.mcs + ip);
+                    }
                 }
-                const float X0 = sv(0), X1 = sv(1), X2 = sv(2);
-                const float Y0 = sv(3), Y1 = sv(4), Y2 = sv(5);
-                const float Z0 = sv(6), Z1 = sv(7), Z2 = sv(8);
-#define QD(a, s0, s1, s2) (a[0] * s0 + a[1] * s1 + a[2] * s2)
-#define QL(a, s0, s1) (a[3] * s0 + a[4] * s1)
-                const float d11x = QD(a11, X0, X1, X2), d12x = QD(a12, X0, X1, X2), d13x = QD(a13, X0, X1, X2);
-                const float d12y = QD(a12, Y0, Y1, Y2), d11y = QD(a11, Y0, Y1, Y2), d13y = QD(a13, Y0, Y1, Y2);
-                const float d13z = QD(a13, Z0, Z1, Z2), d33z = QD(a33, Z0, Z1, Z2);
-                const float q11x = QL(a11, X0, X1), q12x = QL(a12, X0, X1), q13x = QL(a13, X0, X1);
-                const float q12y = QL(a12, Y0, Y1), q11y = QL(a11, Y0, Y1), q13y = QL(a13, Y0, Y1);
-                const float q13z = QL(a13, Z0, Z1), q33z = QL(a33, Z0, Z1);
+#pragma unroll
+                for (int u = 0; u < kCells; ++u) {
+                    if (!ok[u]) continue;
+                    const int t = t0 + u * blockDim.x;
+                    const int p = t / n, z = t - p * n, y = y0 + p;
+                    const long long ip = ipv[u];
+                    const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
+                    auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
+                    float sxx = in[u][0], syy = in[u][1], szz = in[u][2];
+                    if (upd) {
+                        float a11[5], a33[5], a13[5], s5[5], a12[5];
+                        qset_f(in[u][6], in[u][9], in[u][7], w0, inv_w0, a11);
+                        qset_f(in[u][6], in[u][10], in[u][7], w0, inv_w0, a33);
+                        qset_f(in[u][6], in[u][11], in[u][7], w0, inv_w0, a13);
+                        qset_f(in[u][6], in[u][12], in[u][8], w0, inv_w0, s5);
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) {
+                            a12[j] = a11[j] - 2.0f * s5[j];
+                            a13[j] = a13[j] - 2.0f * s5[j];
+                        }
+                        const float X0 = sv(0), X1 = sv(1), X2 = sv(2);
+                        const float Y0 = sv(3), Y1 = sv(4), Y2 = sv(5);
+                        const float Z0 = sv(6), Z1 = sv(7), Z2 = sv(8);
+#define QD(a, s0_, s1_, s2_) (a[0] * s0_ + a[1] * s1_ + a[2] * s2_)
+#define QL(a, s0_, s1_) (a[3] * s0_ + a[4] * s1_)
+                        const float d11x = QD(a11, X0, X1, X2), d12x = QD(a12, X0, X1, X2), d13x = QD(a13, X0, X1, X2);
+                        const float d12y = QD(a12, Y0, Y1, Y2), d11y = QD(a11, Y0, Y1, Y2), d13y = QD(a13, Y0, Y1, Y2);
+                        const float d13z = QD(a13, Z0, Z1, Z2), d33z = QD(a33, Z0, Z1, Z2);
+                        const float q11x = QL(a11, X0, X1), q12x = QL(a12, X0, X1), q13x = QL(a13, X0, X1);
+                        const float q12y = QL(a12, Y0, Y1), q11y = QL(a11, Y0, Y1), q13y = QL(a13, Y0, Y1);
+                        const float q13z = QL(a13, Z0, Z1), q33z = QL(a33, Z0, Z1);
 #undef QD
 #undef QL
-                const float Qxx = q11x + q12y + q13z, Qyy = q12x + q11y + q13z, Qzz = q13x + q13y + q33z;
-                const float Lxx = (Qxx - k.Q[0][ip]) * inv_dt;
-                const float Lyy = (Qyy - k.Q[1][ip]) * inv_dt;
-                const float Lzz = (Qzz - k.Q[2][ip]) * inv_dt;
-                k.Q[0][ip] = Qxx; k.Q[1][ip] = Qyy; k.Q[2][ip] = Qzz;
-                float pxx = 0.f, pxy = 0.f, pxz = 0.f, pyx = 0.f, pyy = 0.f, pyz = 0.f, pzxy = 0.f, pzz = 0.f;
-                auto mem = [&](int m, float dterm, float qterm, float a, float b) {
-                    const float T = dterm + (qterm - k.qn[m][ip]) * inv_dt;
-                    k.qn[m][ip] = qterm;
-                    float ph = k.phn[m][ip];
-                    ph = ph + dt * (-a * ph - b * T);
-                    k.phn[m][ip] = ph;
-                    return ph;
-                };
-                if (in_slab(x, nx, pml)) {
-                    pxx = mem(0, d11x, q11x, k.ax[x], k.bx[x]);
-                    pxy = mem(1, d12x, q12x, k.ax[x], k.bx[x]);
-                    pxz = mem(2, d13x, q13x, k.ax[x], k.bx[x]);
+                        // loss: sum_terms tau-coefficient x (S - S_prev)/dt = (Q - Q_prev)/dt
+                        const float Qxx = q11x + q12y + q13z, Qyy = q12x + q11y + q13z, Qzz = q13x + q13y + q33z;
+                        const float Lxx = (Qxx - in[u][3]) * inv_dt;
+                        const float Lyy = (Qyy - in[u][4]) * inv_dt;
+                        const float Lzz = (Qzz - in[u][5]) * inv_dt;
+                        q0[ip] = Qxx; q1[ip] = Qyy; q2[ip] = Qzz;
+                        float pxx = 0.f, pxy = 0.f, pxz = 0.f, pyx = 0.f, pyy = 0.f, pyz = 0.f, pzxy = 0.f, pzz = 0.f;
+                        auto mem = [&](int m, float dterm, float qterm, float a, float b) {
+                            const float T = dterm + (qterm - k.qn[m][ip]) * inv_dt;
+                            k.qn[m][ip] = qterm;
+                            float ph = k.phn[m][ip];
+                            ph = ph + dt * (-a * ph - b * T);
+                            k.phn[m][ip] = ph;
+                            return ph;
+                        };
+                        if (in_slab(x, nx, pml)) {
+                            pxx = mem(0, d11x, q11x, k.ax[x], k.bx[x]);
+                            pxy = mem(1, d12x, q12x, k.ax[x], k.bx[x]);
+                            pxz = mem(2, d13x, q13x, k.ax[x], k.bx[x]);
+                        }
+                        if (in_slab(y, ny, pml)) {
+                            pyx = mem(3, d12y, q12y, k.ay[y], k.by[y]);
+                            pyy = mem(4, d11y, q11y, k.ay[y], k.by[y]);
+                            pyz = mem(5, d13y, q13y, k.ay[y], k.by[y]);
+                        }
+                        if (in_slab(z, n, pml)) {
+                            pzxy = mem(6, d13z, q13z, k.az[z], k.bz[z]);  // phi_vz_zx == phi_vz_zy
+                            pzz = mem(7, d33z, q33z, k.az[z], k.bz[z]);
+                        }
+                        sxx = sxx + dt * (d11x + d12y + d13z + Lxx + pxx + pyx + pzxy);
+                        syy = syy + dt * (d12x + d11y + d13z + Lyy + pxy + pyy + pzxy);
+                        szz = szz + dt * (d13x + d13y + d33z + Lzz + pxz + pyz + pzz);
+                    }
+                    if (ip == src_ip && it < k.nt_rec) {  // cu:772-777, after the update
+                        if (k.src_type == 1) {
+                            const float w = k.rik[it];
+                            sxx += w; syy += w; szz += w;
+                        } else {
+                            k.v[0][ip] += k.rik[it];
+                        }
+                    }
+                    if (upd || ip == src_ip) { s0[ip] = sxx; s1[ip] = syy; s2[ip] = szz; }
+                    D[(0 * P + p) * np1 + z] = szz;
                 }
-                if (in_slab(y, ny, pml)) {
-                    pyx = mem(3, d12y, q12y, k.ay[y], k.by[y]);
-                    pyy = mem(4, d11y, q11y, k.ay[y], k.by[y]);
-                    pyz = mem(5, d13y, q13y, k.ay[y], k.by[y]);
-                }
-                if (in_slab(z, n, pml)) {
-                    pzxy = mem(6, d13z, q13z, k.az[z], k.bz[z]);
-                    pzz = mem(7, d33z, q33z, k.az[z], k.bz[z]);
-                }
-                sxx = sxx + dt * (d11x + d12y + d13z + Lxx + pxx + pyx + pzxy);
-                syy = syy + dt * (d12x + d11y + d13z + Lyy + pxy + pyy + pzxy);
-                szz = szz + dt * (d13x + d13y + d33z + Lzz + pxz + pyz + pzz);
-            }
-            if (ip == src_ip && it < k.nt_rec) {
-                if (k.src_type == 1) {
-                    const float w = k.rik[it];
-                    sxx += w; syy += w; szz += w;
-                } else {
-                    k.v[0][ip] += k.rik[it];
-                }
-            }
-            if (upd || ip == src_ip) { k.s[0][ip] = sxx; k.s[1][ip] = syy; k.s[2][ip] = szz; }
-            out = szz;
-        } else {
-            constexpr int sidx = GRP == 1 ? 4 : GRP == 2 ? 3 : 5;  // sxz, sxy, syz in s[]
-            float sig = k.s[sidx][ip];
-            if (upd) {
-                float mu[5];
+            } else {
+                const int sidx = grp == 1 ? 4 : grp == 2 ? 3 : 5;  // sxz, sxy, syz in s[]
+                float* __restrict__ sg = k.s[sidx];
+                float* __restrict__ qg = k.Q[sidx];
+                float in[kCells][7];
+                long long ipv[kCells];
+                bool ok[kCells];
 #pragma unroll
-                for (int j = 0; j < 5; ++j) mu[j] = k.MU[j][ip];
-                const float A0 = sv(0), A1 = sv(1), A2 = sv(2), B0 = sv(3), B1 = sv(4), B2 = sv(5);
-                const float dA = mu[0] * A0 + mu[1] * A1 + mu[2] * A2, qA = mu[3] * A0 + mu[4] * A1;
-                const float dB = mu[0] * B0 + mu[1] * B1 + mu[2] * B2, qB = mu[3] * B0 + mu[4] * B1;
-                const float Qs = qA + qB;
-                const float L = (Qs - k.Q[sidx][ip]) * inv_dt;
-                k.Q[sidx][ip] = Qs;
-                // term A: GRP1 vx_z (z slab), GRP2 vx_y (y slab), GRP3 vy_z (z slab)
-                // term B: GRP1 vz_x (x slab), GRP2 vy_x (x slab), GRP3 vz_y (y slab)
-                const int mA = (GRP - 1) * 2, mB = mA + 1;
-                auto mem = [&](int m, float dterm, float qterm, float a, float b) {
-                    const float T = dterm + (qterm - k.qs[m][ip]) * inv_dt;
-                    k.qs[m][ip] = qterm;
-                    float ph = k.phs[m][ip];
-                    ph = ph + dt * (-a * ph - b * T);
-                    k.phs[m][ip] = ph;
-                    return ph;
-                };
-                float phA = 0.f, phB = 0.f;
-                if (GRP == 1) {
-                    if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
-                    if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
-                } else if (GRP == 2) {
-                    if (in_slab(y, ny, pml)) phA = mem(mA, dA, qA, k.ayh[y], k.byh[y]);
-                    if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
-                } else {
-                    if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
-                    if (in_slab(y, ny, pml)) phB = mem(mB, dB, qB, k.ayh[y], k.byh[y]);
+                for (int u = 0; u < kCells; ++u) {
+                    const int t = t0 + u * blockDim.x;
+                    ok[u] = t < P * n;
+                    const int p = t / n, z = t - p * n;
+                    ipv[u] = cell(k, x, y0 + p, z);
+                    if (ok[u]) {
+                        const long long ip = ipv[u];
+                        in[u][0] = sg[ip];
+                        in[u][1] = qg[ip];
+#pragma unroll
+                        for (int j = 0; j < 5; ++j) in[u][2 + j] = __ldg(k.MU[j] + ip);
+                    }
                 }
-                sig = sig + dt * (dA + phA + dB + phB + L);
-                k.s[sidx][ip] = sig;
+#pragma unroll
+                for (int u = 0; u < kCells; ++u) {
+                    if (!ok[u]) continue;
+                    const int t = t0 + u * blockDim.x;
+                    const int p = t / n, z = t - p * n, y = y0 + p;
+                    const long long ip = ipv[u];
+                    const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
+                    auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
+                    float sig = in[u][0];
+                    if (upd) {
+                        const float* mu = &in[u][2];
+                        const float A0 = sv(0), A1 = sv(1), A2 = sv(2), B0 = sv(3), B1 = sv(4), B2 = sv(5);
+                        const float dA = mu[0] * A0 + mu[1] * A1 + mu[2] * A2, qA = mu[3] * A0 + mu[4] * A1;
+                        const float dB = mu[0] * B0 + mu[1] * B1 + mu[2] * B2, qB = mu[3] * B0 + mu[4] * B1;
+                        const float Qs = qA + qB;
+                        const float L = (Qs - in[u][1]) * inv_dt;
+                        qg[ip] = Qs;
+                        // term A: xz vx_z (z slab), xy vx_y (y slab), yz vy_z (z slab)
+                        // term B: xz vz_x (x slab), xy vy_x (x slab), yz vz_y (y slab)
+                        const int mA = (grp - 1) * 2, mB = mA + 1;
+                        auto mem = [&](int m, float dterm, float qterm, float a, float b) {
+                            const float T = dterm + (qterm - k.qs[m][ip]) * inv_dt;
+                            k.qs[m][ip] = qterm;
+                            float ph = k.phs[m][ip];
+                            ph = ph + dt * (-a * ph - b * T);
+                            k.phs[m][ip] = ph;
+                            return ph;
+                        };
+                        float phA = 0.f, phB = 0.f;
+                        if (grp == 1) {
+                            if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
+                            if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
+                        } else if (grp == 2) {
+                            if (in_slab(y, ny, pml)) phA = mem(mA, dA, qA, k.ayh[y], k.byh[y]);
+                            if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
+                        } else {
+                            if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
+                            if (in_slab(y, ny, pml)) phB = mem(mB, dB, qB, k.ayh[y], k.byh[y]);
+                        }
+                        sig = sig + dt * (dA + phA + dB + phB + L);
+                        sg[ip] = sig;
+                    }
+                    if (grp == 1) D[(1 * P + p) * np1 + z] = sig;
+                    if (grp == 3) D[(2 * P + p) * np1 + z] = sig;
+                }
             }
-            out = sig;
         }
-        S[p * np1 + z] = out;  // S[0][p][z]
+        __syncthreads();
     }
-    if constexpr (GRP == 2) return;
-    __syncthreads();
 
-    // 3. z derivative of the updated stress: GRP0 dz- szz -> R_z, GRP1 dz+ sxz
-    //    -> R_x, GRP3 dz+ syz -> R_y (cu:1279-1306 partz2, partz1, partz3).
+    // 3. z derivatives of the new szz (backward shift -> R_z), sxz (forward ->
+    //    R_x), syz (forward -> R_y), batched: pencil p' = f*Qp + q.
     {
-        const float2* T = GRP == 0 ? k.Bz : k.Fz;
-        const int rc = GRP == 0 ? 2 : GRP == 1 ? 0 : 1;
-        const int phm = GRP == 0 ? 8 : GRP == 1 ? 2 : 5;  // php: pzz_z, pxz_z, pyz_z
+        const int npen = 3 * Qp;
         const float inv_n = 1.0f / n;
-        auto load = [&](int q, int i) -> float2 { return make_float2(S[(2 * q) * np1 + i], S[(2 * q + 1) * np1 + i]); };
+        auto load = [&](int pp, int i) -> float2 {
+            const int f = pp / Qp, q = pp - f * Qp;
+            return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
+        };
         float2* Zf = fft_out_buf(k.pz, A, B);
-        auto store_f = [&](int q, int i, float2 v) { Zf[q * np1 + i] = v; };
-        fft_run<false>(k.pz, tw, A, B, Qp, np1, 1, false, load, store_f);
+        auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
+        fft_run<false>(k.pz, tw, A, B, npen, np1, 1, false, load, store_f);
         float2* X1 = Zf == A ? B : A;
-        auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[q * np1 + i], cscale(T[i], inv_n)); };
-        auto store_i = [&](int q, int i, float2 v) {
+        auto load_i = [&](int pp, int i) -> float2 {
+            const int f = pp / Qp;
+            return cmul(Zf[pp * np1 + i], cscale(f == 0 ? k.Bz[i] : k.Fz[i], inv_n));
+        };
+        auto store_i = [&](int pp, int i, float2 v) {
+            const int f = pp / Qp, q = pp - f * Qp;
+            const int rc = f == 0 ? 2 : f == 1 ? 0 : 1;
+            const int phm = f == 0 ? 8 : f == 1 ? 2 : 5;  // php: pzz_z, pxz_z, pyz_z
             const bool zin = i < n - 1 && x < nx - 1;
             const bool zslab = in_slab(i, n, pml);
 #pragma unroll
@@ -346,8 +480,8 @@ __global__ void __launch_bounds__(kThreads) k_iz(KP k, int P)
                 float r = part;
                 if (zslab && zin && y < ny - 1) {
                     float ph = k.php[phm][ip];
-                    const float a = GRP == 0 ? k.azh[i] : k.az[i];
-                    const float b = GRP == 0 ? k.bzh[i] : k.bz[i];
+                    const float a = f == 0 ? k.azh[i] : k.az[i];
+                    const float b = f == 0 ? k.bzh[i] : k.bz[i];
                     ph = ph + dt * (-a * ph - b * part);
                     k.php[phm][ip] = ph;
                     r += ph;
@@ -355,7 +489,7 @@ __global__ void __launch_bounds__(kThreads) k_iz(KP k, int P)
                 k.R[rc][ip] = r;
             }
         };
-        fft_run<false>(k.pz, tw, X1, Zf, Qp, np1, 1, true, load_i, store_i);
+        fft_run<false>(k.pz, tw, X1, Zf, npen, np1, 1, true, load_i, store_i);
     }
 }
 
@@ -371,7 +505,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
     float2* tF = tw + n;
     float2* tB = tF + n;
     float2* A = tB + n;
-    float2* B = A + n * P;
+    float2* B = A + (n + n / 16) * P;
     load_table(tw, k.tw_y, n);
     load_table(tF, k.Fy, n);
     load_table(tB, k.By, n);
@@ -392,7 +526,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
             return make_float2(sxy[ip], syy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_run<true>(k.py, tw, A, B, P, 1, P, false, load, store);
+        fft_run<true>(k.py, tw, A, B, P, 1, P, false, load, store, 4);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
@@ -415,7 +549,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
             k.R[0][ip] += rx;
             k.R[1][ip] += ry;
         };
-        fft_run<true>(k.py, tw, X1, Zf, P, 1, P, true, load_i, store_i);
+        fft_run<true>(k.py, tw, X1, Zf, P, 1, P, true, load_i, store_i, 4);
     }
     // pass 2: syz, pencils (2q, 2q+1)
     {
@@ -426,7 +560,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
             return *reinterpret_cast<const float2*>(syz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_run<true>(k.py, tw, A, B, Qp, 1, Qp, false, load, store);
+        fft_run<true>(k.py, tw, A, B, Qp, 1, Qp, false, load, store, 4);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
@@ -445,7 +579,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
                 k.R[2][ip] += r;
             }
         };
-        fft_run<true>(k.py, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i);
+        fft_run<true>(k.py, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i, 4);
     }
 }
 
@@ -461,7 +595,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
     float2* tF = tw + n;
     float2* tB = tF + n;
     float2* A = tB + n;
-    float2* B = A + n * P;
+    float2* B = A + (n + n / 16) * P;
     load_table(tw, k.tw_x, n);
     load_table(tF, k.Fx, n);
     load_table(tB, k.Bx, n);
@@ -481,7 +615,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
             return make_float2(sxx[ip], sxy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store);
+        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store, 4);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
@@ -505,7 +639,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
             k.v[0][ip] += dt * k.rinv[0][ip] * (px + k.R[0][ip]);
             k.v[1][ip] += dt * k.rinv[1][ip] * (py + k.R[1][ip]);
         };
-        fft_run<true>(k.px, tw, X1, Zf, P, 1, P, true, load_i, store_i);
+        fft_run<true>(k.px, tw, X1, Zf, P, 1, P, true, load_i, store_i, 4);
     }
     // pass 2: sxz pencils (2q, 2q+1) -> vz
     {
@@ -516,7 +650,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_run<true>(k.px, tw, A, B, Qp, 1, Qp, false, load, store);
+        fft_run<true>(k.px, tw, A, B, Qp, 1, Qp, false, load, store, 4);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
@@ -536,7 +670,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
                 k.v[2][ip] += dt * k.rinv[2][ip] * (part + k.R[2][ip]);
             }
         };
-        fft_run<true>(k.px, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i);
+        fft_run<true>(k.px, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i, 4);
     }
 }
 
@@ -568,35 +702,41 @@ __device__ __forceinline__ void qset(double v, double g, double r, double w0, do
     o[4] = r * c * c * g * g * pi / w0;
 }
 
-// coef layout: [0..5) K11, [5..10) K12, [10..15) K13, [15..20) K33, [20..25) S.
+// Per-cell coefficient build, FP64.  out[0..7): rho, gamma_p, gamma_s and the
+// effective velocities c = v cos(pi gamma / 2) of c11, c33, c13 (gamma_p) and
+// c44 (gamma_s); out[7..12): the S set of c44, input of the 8-point average.
+// VTI (project extension): c33 = rho vp^2, c44 = c66 = rho vs^2,
+// c11 = c33 (1 + 2 eps), c13 = sqrt((c33 - c44)(c33 (1 + 2 delta) - c44)) - c44,
+// each modulus taking the constant-Q set of its effective velocity
+// (v11 = vp sqrt(1 + 2 eps), v13 = sqrt((c13 + 2 c44)/rho)); the off-diagonal
+// sets are P(v) - 2 S(vs), which at eps = delta = 0 is the reference's
+// eta_p - 2 eta_s (cu:851-898).
 __global__ void k_coef(long long ntp, const float* velp, const float* vels, const float* rho, const float* gp,
                        const float* gs, const float* eps, const float* delta, int vti, double w0, float* const* out)
 {
+    const double pi = 3.1415926;
     for (long long ip = blockIdx.x * (long long)blockDim.x + threadIdx.x; ip < ntp;
          ip += (long long)gridDim.x * blockDim.x) {
         const double r = rho[ip], vp = velp[ip], vs = vels[ip], g_p = gp[ip], g_s = gs[ip];
-        double s5[5], p33[5], p11[5], p13[5];
-        qset(vs, g_s, r, w0, s5);
-        qset(vp, g_p, r, w0, p33);
+        const double cp = cos(g_p * pi / 2.0), cq = cos(g_s * pi / 2.0);
+        double v11 = vp, v13 = vp;
         if (vti) {
-            // VTI (project extension): c33 = rho vp^2, c44 = c66 = rho vs^2,
-            // c11 = c33 (1 + 2 eps), c13 = sqrt((c33-c44)(c33(1+2 delta)-c44)) - c44;
-            // each modulus gets the constant-Q set of its effective velocity.
             const double e = eps[ip], dl = delta[ip];
             const double c33 = r * vp * vp, c44 = r * vs * vs;
             const double c13 = sqrt((c33 - c44) * (c33 * (1.0 + 2.0 * dl) - c44)) - c44;
-            qset(vp * sqrt(1.0 + 2.0 * e), g_p, r, w0, p11);
-            qset(sqrt((c13 + 2.0 * c44) / r), g_p, r, w0, p13);
-        } else {
-            for (int j = 0; j < 5; ++j) { p11[j] = p33[j]; p13[j] = p33[j]; }
+            v11 = vp * sqrt(1.0 + 2.0 * e);
+            v13 = sqrt((c13 + 2.0 * c44) / r);
         }
-        for (int j = 0; j < 5; ++j) {
-            out[j][ip] = (float)p11[j];
-            out[5 + j][ip] = (float)(p11[j] - 2.0 * s5[j]);
-            out[10 + j][ip] = (float)(p13[j] - 2.0 * s5[j]);
-            out[15 + j][ip] = (float)p33[j];
-            out[20 + j][ip] = (float)s5[j];
-        }
+        out[0][ip] = (float)r;
+        out[1][ip] = (float)g_p;
+        out[2][ip] = (float)g_s;
+        out[3][ip] = (float)(v11 * cp);
+        out[4][ip] = (float)(vp * cp);
+        out[5][ip] = (float)(v13 * cp);
+        out[6][ip] = (float)(vs * cq);
+        double s5[5];
+        qset(vs, g_s, r, w0, s5);
+        for (int j = 0; j < 5; ++j) out[7 + j][ip] = (float)s5[j];
     }
 }
 
@@ -671,6 +811,70 @@ __global__ void k_deriv1d(KP k, int axis, int fwd, const float* in, float* out, 
     fft_run<true>(pl, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i);
 }
 
+// ------------------------------------------- single-field constant-Q field --
+// One of the 27 stress-side fields on its own: out = Re IFFT3(|k|^pw T(k_a)
+// FFT3(in)) / ntp with T the forward or backward staggered shift along axis
+// a (cu:475-744 with the transforms around them).  The half spectrum H[0]
+// (kz-major, as in the step) is the scratch; k_fz and k_cy do the z and y
+// passes, these two kernels the k-space x pass and the C2R along z.
+__global__ void __launch_bounds__(kThreads) kq_mx(KP k, int P, int axis, int fwd, int pw)
+{
+    extern __shared__ float4 smem4[];
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    const int n = k.nx;
+    float2* tw = sm;
+    float2* V = tw + n;   // [n][P]
+    float2* A = V + n * P;
+    float2* B = A + n * P;
+    load_table(tw, k.tw_x, n);
+    __syncthreads();
+    const int kz = blockIdx.y, y0 = blockIdx.x * P;
+    float2* H = k.H[0];
+    auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
+    auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
+    fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store);
+    const float kz2 = k.kz[kz] * k.kz[kz];
+    auto load_i = [&](int p, int i) -> float2 {
+        const float kyv = k.ky[y0 + p], kxv = k.kx[i];
+        const float k2 = fmaxf(kxv * kxv + kyv * kyv + kz2, 1e-10f);
+        const float ap = pw == 0 ? 1.0f : (pw < 0 ? 1.0f / sqrtf(k2) : sqrtf(k2));
+        float2 T;
+        if (axis == 0) T = fwd ? k.Fx[i] : k.Bx[i];
+        else if (axis == 1) T = fwd ? k.Fy[y0 + p] : k.By[y0 + p];
+        else T = fwd ? k.Fz[kz] : k.Bz[kz];
+        return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
+    };
+    auto store_i = [&](int p, int i, float2 v) { H[spec(k, kz, i, y0 + p)] = v; };
+    fft_run<true>(k.px, tw, A, B, P, 1, P, true, load_i, store_i);
+}
+
+__global__ void __launch_bounds__(kThreads) kq_iz(KP k, int P, float* out)
+{
+    extern __shared__ float4 smem4[];
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    const int n = k.nz, Qp = P / 2;
+    float2* tw = sm;
+    float2* A = tw + n;
+    float2* B = A + Qp * n;
+    load_table(tw, k.tw_z, n);
+    __syncthreads();
+    const int x = blockIdx.y, y0 = blockIdx.x * P;
+    const float2* g = k.H[0];
+    auto load = [&](int q, int i) -> float2 {
+        const int kk = i <= n / 2 ? i : n - i;
+        const float4 gg = *reinterpret_cast<const float4*>(g + spec(k, kk, x, y0 + 2 * q));
+        float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
+        if (kk == 0 || 2 * kk == n) { a.y = 0.f; b.y = 0.f; }
+        if (i > n / 2) { a.y = -a.y; b.y = -b.y; }
+        return make_float2(a.x - b.y, a.y + b.x);
+    };
+    auto store = [&](int q, int i, float2 v) {
+        out[cell(k, x, y0 + 2 * q, i)] = v.x;
+        out[cell(k, x, y0 + 2 * q + 1, i)] = v.y;
+    };
+    fft_run<true>(k.pz, tw, A, B, Qp, 1, Qp, true, load, store);
+}
+
 // --------------------------------------------------------- tile selection --
 int tile_of(int n, int want)
 {
@@ -680,13 +884,22 @@ int tile_of(int n, int want)
 }
 
 size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + 1)); }
-size_t smem_cy(const KP& k, int L) { return sizeof(float2) * (k.ny + 2 * L * (k.ny + 1)); }
-size_t smem_mx(const KP& k, int P) { return sizeof(float2) * (3 * k.nx + 5 * k.nx * P) + sizeof(float) * k.nx; }
-size_t smem_iz(const KP& k, int P, int nf)
+size_t smem_cy(const KP& k, int L) { return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16)); }
+size_t smem_mx(const KP& k, int P)
 {
-    return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + 1)) + sizeof(float) * nf * P * (k.nz + 1);
+    return sizeof(float2) * (3 * k.nx + k.nx * P + 2 * (k.nx + k.nx / 16) * P) + sizeof(float) * k.nx;
 }
-size_t smem_vyx(int n, int P) { return sizeof(float2) * (3 * n + 2 * n * P); }
+// k_sigma layout: tw[nz] | A | B (only when the z transform has more than two
+// stages; otherwise B aliases S, used only by the final z-derivative pass) |
+// S[9][P][nz+1] | D[3][P][nz+1].
+size_t smem_sigma(const KP& k, int P)
+{
+    const size_t bufA = (size_t)9 * (P / 2) * k.nz;
+    const int nb = k.pz.nst > 2 ? 2 : 1;
+    return sizeof(float2) * (k.nz + nb * bufA) + sizeof(float) * (size_t)12 * P * (k.nz + 1);
+}
+
+size_t smem_vyx(int n, int P) { return sizeof(float2) * (3 * n + 2 * (n + n / 16) * P); }
 
 }  // namespace
 
@@ -702,34 +915,60 @@ int configure_kernels()
     set((const void*)k_cy<false>);
     set((const void*)k_cy<true>);
     set((const void*)k_mx);
-    set((const void*)k_iz<0>);
-    set((const void*)k_iz<1>);
-    set((const void*)k_iz<2>);
-    set((const void*)k_iz<3>);
+    set((const void*)k_sigma);
     set((const void*)k_vy);
     set((const void*)k_vx);
     set((const void*)k_deriv1d);
+    set((const void*)kq_mx);
+    set((const void*)kq_iz);
     return (int)e;
 }
 
-void launch_step(const KP& k, cudaStream_t st)
+const char* const kStepKernelNames[kStepKernels] = {"k_vy",  "k_vx",     "k_fz",    "k_cy_fwd",
+                                                     "k_mx",  "k_cy_inv", "k_sigma", "k_rec"};
+
+// One time step.  With a profile sink, an event is recorded before the first
+// kernel and after every launch, tagged with the launch's kernel index.
+void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
 {
+    auto mark = [&](int kind) {
+        if (prof && prof->n < StepProfile::kMax) {
+            cudaEventRecord(prof->ev[prof->n], st);
+            prof->kind[prof->n++] = kind;
+        }
+    };
+    mark(-1);
     const int Pv = tile_of(k.nz, 16);
     k_vy<<<dim3(k.nz / Pv, k.nx), kThreads, smem_vyx(k.ny, Pv), st>>>(k, Pv);
+    mark(0);
     k_vx<<<dim3(k.nz / Pv, k.ny), kThreads, smem_vyx(k.nx, Pv), st>>>(k, Pv);
+    mark(1);
     const int Pz = tile_of(k.ny, 16);
     k_fz<<<dim3(k.ny / Pz, k.nx, 3), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
-    const int L = tile_of(k.nkz * k.nx, 8) > 1 ? tile_of(k.nx, 8) : 1;
-    k_cy<false><<<dim3(k.nkz * k.nx / L, 3), kThreads, smem_cy(k, L), st>>>(k, L);
-    const int Pm = tile_of(k.ny, 8);
-    k_mx<<<dim3(k.ny / Pm, k.nkz), kThreads, smem_mx(k, Pm), st>>>(k, Pm);
-    k_cy<true><<<dim3(k.nkz * k.nx / L, kNumG), kThreads, smem_cy(k, L), st>>>(k, L);
-    const int Pi = tile_of(k.ny, 8);
-    k_iz<0><<<dim3(k.ny / Pi, k.nx), kThreads, smem_iz(k, Pi, 9), st>>>(k, Pi);
-    k_iz<1><<<dim3(k.ny / Pi, k.nx), kThreads, smem_iz(k, Pi, 6), st>>>(k, Pi);
-    k_iz<2><<<dim3(k.ny / Pi, k.nx), kThreads, smem_iz(k, Pi, 6), st>>>(k, Pi);
-    k_iz<3><<<dim3(k.ny / Pi, k.nx), kThreads, smem_iz(k, Pi, 6), st>>>(k, Pi);
-    if (k.rn > 0) k_rec<<<(k.rn + 255) / 256, 256, 0, st>>>(k);
+    mark(2);
+    // k-space passes in batches of kz planes: the 27 spectra a batch's k_mx
+    // writes are read back by its k_cy<true> while still in L2 (a batch is
+    // sized to ~48 MB of spectra), so they reach HBM once instead of twice.
+    const int L = tile_of(k.nx, 8);
+    const int Pm = tile_of(k.ny, 16);
+    const int batch = k.kz_batch > 0 ? k.kz_batch : k.nkz;
+    for (int kz0 = 0; kz0 < k.nkz; kz0 += batch) {
+        const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
+        const long long line0 = (long long)kz0 * k.nx;
+        k_cy<false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+        mark(3);
+        k_mx<<<dim3(k.ny / Pm, nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
+        mark(4);
+        k_cy<true><<<dim3(nb * k.nx / L, kNumG), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+        mark(5);
+    }
+    const int Ps = tile_of(k.ny, 4);
+    k_sigma<<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
+    mark(6);
+    if (k.rn > 0) {
+        k_rec<<<(k.rn + 255) / 256, 256, 0, st>>>(k);
+        mark(7);
+    }
 }
 
 void launch_coef_build(const KP& k, const float* velp, const float* vels, const float* rho, const float* gp,
@@ -746,6 +985,20 @@ void launch_mu_rinv(const KP& k, const float* rho, const float* const* sset, cud
     a.rho = rho;
     for (int c = 0; c < 3; ++c) a.rinv[c] = const_cast<float*>(k.rinv[c]);
     k_mu_rinv<<<148 * 8, 256, 0, st>>>(k, a);
+}
+
+// k.v[0] = input field, k.H[0] = k.G[0] = half-spectrum scratch (nkz*nx*ny).
+void launch_q_derivative(const KP& k, int axis, int fwd, int pw, float* out, cudaStream_t st)
+{
+    const int Pz = tile_of(k.ny, 16);
+    k_fz<<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
+    const int L = tile_of(k.nx, 8);
+    k_cy<false><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    const int Pm = tile_of(k.ny, 8);
+    kq_mx<<<dim3(k.ny / Pm, k.nkz), kThreads, sizeof(float2) * (k.nx + 3 * k.nx * Pm), st>>>(k, Pm, axis, fwd, pw);
+    k_cy<true><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    const int Pi = tile_of(k.ny, 8);
+    kq_iz<<<dim3(k.ny / Pi, k.nx), kThreads, sizeof(float2) * (k.nz + 2 * (Pi / 2) * k.nz), st>>>(k, Pi, out);
 }
 
 void launch_derivative_1d(const KP& k, int axis, int fwd, const float* in, float* out, cudaStream_t st)

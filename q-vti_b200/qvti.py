@@ -66,6 +66,8 @@ def lib():
                                                  ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int, _I,
                                                  _I, ctypes.c_int, _F, _F, _F]),
             "qvti_derivative_1d": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _F, _F]),
+            "qvti_q_derivative": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F, _F]),
+            "qvti_profile_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _I, ctypes.c_char_p, _F, _D]),
             "qvti_last_error": (ctypes.c_int, []),
             "qvti_error_string": (ctypes.c_char_p, [ctypes.c_int]),
         }
@@ -195,6 +197,26 @@ class Simulation:
         bad = ctypes.c_int(0)
         rc = lib().qvti_field_norms(self._h, out.ctypes.data_as(_D), ctypes.byref(bad))
         return out, bool(bad.value), rc
+
+    def profile_step(self, nrep=3):
+        """Per-kernel device time of one step: list of (name, ms, algorithmic bytes)."""
+        maxk = 32
+        names = ctypes.create_string_buffer(32 * maxk)
+        ms = np.zeros(maxk, np.float32)
+        by = np.zeros(maxk, np.float64)
+        nk = ctypes.c_int(0)
+        _check(lib().qvti_profile_step(self._h, int(nrep), maxk, ctypes.byref(nk), names, _fp(ms), by.ctypes.data_as(_D)),
+               "qvti_profile_step")
+        raw = names.raw
+        return [(raw[32 * i:32 * i + 32].split(b"\0")[0].decode(), float(ms[i]), float(by[i])) for i in range(nk.value)]
+
+    def q_derivative(self, field, axis, forward, power):
+        """Re IFFT3(|k|^power T_axis FFT3(field)) / ntp (one constant-Q field)."""
+        f = _f32(field)
+        out = np.zeros_like(f)
+        _check(lib().qvti_q_derivative(self._h, int(axis), 1 if forward else 0, int(power), _fp(f), _fp(out)),
+               "qvti_q_derivative")
+        return out
 
     def derivative_1d(self, field, axis, forward):
         f = _f32(field)

@@ -31,3 +31,34 @@ def test_derivative_1d(qvti, oracle, shape, axis, forward):
     ref = _numpy_derivative(f, axis, d[axis], forward, oracle)
     err = np.abs(out - ref).max() / np.abs(ref).max()
     assert err < 2e-5, err
+
+
+def _numpy_q_derivative(f, d, axis, forward, power, oracle):
+    """Re IFFT3(|k|^power T(k_axis) FFT3(f)) in FP64 (cuviscoelas_3D.cu:188-190, 475-744)."""
+    n = f.shape
+    ks = [oracle.wavenumbers(n[a], d[a]) for a in range(3)]
+    k2 = ks[0][:, None, None] ** 2 + ks[1][None, :, None] ** 2 + ks[2][None, None, :] ** 2
+    k2[0, 0, 0] = 1e-10
+    ap = k2 ** (0.5 * power)
+    fw, bw = oracle.shift_tables(n[axis], d[axis])
+    T = (fw if forward else bw).copy()
+    if n[axis] % 2 == 0:
+        T[n[axis] // 2] = T[n[axis] // 2].real
+    sh = [1, 1, 1]
+    sh[axis] = n[axis]
+    F = np.fft.fftn(f.astype(np.float64))
+    return np.real(np.fft.ifftn(F * ap * T.reshape(sh)))
+
+
+@pytest.mark.parametrize("power", [-1, 0, 1])
+@pytest.mark.parametrize("axis,forward", [(0, True), (1, False), (2, True), (2, False)])
+def test_q_derivative(qvti, oracle, power, axis, forward):
+    shape = (32, 48, 64)
+    d = (10.0, 12.5, 8.0)
+    rng = np.random.default_rng(3 + power + 5 * axis)
+    f = rng.standard_normal(shape).astype(np.float32)
+    with qvti.Simulation(*shape, 6, *d, 1e-3, 20.0) as sim:
+        out = sim.q_derivative(f, axis, forward, power)
+    ref = _numpy_q_derivative(f, d, axis, forward, power, oracle)
+    err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+    assert err < 1e-5, err
