@@ -136,6 +136,27 @@ int qvti_derivative_1d(qvti_sim* sim, int axis, int fwd, const float* in, float*
  * cuviscoelas_3D.cu:1342-1562 on its own.  For tests and diagnostics. */
 int qvti_q_derivative(qvti_sim* sim, int axis, int fwd, int power, const float* in, float* out);
 
+/* qvti_q_derivative for callers that cannot allocate device memory: a
+ * serving process with a footprint fixed at start-up, a host framework that
+ * hands out pre-planned buffers from its own pool, or a latency-critical loop
+ * that cannot absorb the device-wide synchronisation of cudaMalloc/cudaFree.
+ * No counterpart in the reference.
+ *   d_in, d_out: device arrays of ntx*nty*ntz floats (caller-owned); the
+ *   result is written to d_out asynchronously on `stream` (a cudaStream_t,
+ *   NULL for the default stream).
+ * Nothing is allocated: the scratch half spectrum and the 1D tables live in
+ * fixed-size device arrays of the library, held by every GPU that loads it
+ * until the process exits.  Limits: each dimension even, 16..1024 and
+ * 2/3/5/7-smooth, and (ntz/2 + 1)*ntx*nty <= 524288 (4 MiB of scratch, e.g.
+ * 96^3 or 64x64x128); larger grids return QVTI_ERR_UNSUPPORTED.  The first
+ * call on a device looks up the arrays' device addresses (and sets kernel
+ * attributes) -- make it before any stream capture.  All calls on a device
+ * share one scratch, which keeps the last call's contents (nothing in it
+ * needs clearing): calls that can overlap on the GPU (different streams,
+ * no ordering between them) race and must not be issued. */
+int qvti_q_derivative_noalloc(const float* d_in, float* d_out, int ntx, int nty, int ntz, float dx, float dy,
+                              float dz, int axis, int fwd, int power, void* stream);
+
 /* Per-kernel device time of the time step: runs nrep steps (advancing the
  * state) with CUDA events between their kernels; sets *nkernels to the
  * kernels per step and fills names (maxk*32 chars), the average ms per launch

@@ -135,6 +135,14 @@ __global__ void k_norms(long long ntp, const float* f, double* out, int* nonfini
 
 }  // namespace
 
+bool make_fft_plan(int n, FftPlan* p) { return make_plan(n, p); }
+
+void launch_axis_tables(int n, double d, double f0, int pml, float2* tw, float* kmag, float2* F, float2* B,
+                        float* a, float* b, float* ah, float* bh, cudaStream_t st)
+{
+    k_axis_tables<<<4, 256, 0, st>>>(n, d, f0, pml, tw, kmag, F, B, a, b, ah, bh);
+}
+
 struct Sim {
     qvti_config cfg{};
     int nx = 0, ny = 0, nz = 0, nkz = 0;

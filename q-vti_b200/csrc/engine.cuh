@@ -94,6 +94,11 @@ void launch_coef_build(const KP& kp, const float* velp, const float* vels, const
 void launch_mu_rinv(const KP& kp, const float* rho, const float* const* sset, cudaStream_t st);
 int configure_kernels();   // raise dynamic shared-memory limits, returns cudaError_t
 
+// Radix plan of a transform length; FP64 build of one axis's 1D tables.
+bool make_fft_plan(int n, FftPlan* p);
+void launch_axis_tables(int n, double d, double f0, int pml, float2* tw, float* kmag, float2* F, float2* B,
+                        float* a, float* b, float* ah, float* bh, cudaStream_t st);
+
 // Individual stages, exposed for unit tests through the C ABI.
 void launch_q_derivative(const KP& kp, int axis, int fwd, int pw, float* out, cudaStream_t st);
 void launch_derivative_1d(const KP& kp, int axis, int fwd_shift, const float* in, float* out, cudaStream_t st);

@@ -67,6 +67,9 @@ def lib():
                                                  _I, ctypes.c_int, _F, _F, _F]),
             "qvti_derivative_1d": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _F, _F]),
             "qvti_q_derivative": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F, _F]),
+            "qvti_q_derivative_noalloc": (ctypes.c_int, [_V, _V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                         ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                                         ctypes.c_int, ctypes.c_int, ctypes.c_int, _V]),
             "qvti_profile_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _I, ctypes.c_char_p, _F, _D]),
             "qvti_last_error": (ctypes.c_int, []),
             "qvti_error_string": (ctypes.c_char_p, [ctypes.c_int]),
@@ -224,6 +227,17 @@ class Simulation:
         _check(lib().qvti_derivative_1d(self._h, int(axis), 1 if forward else 0, _fp(f), _fp(out)),
                "qvti_derivative_1d")
         return out
+
+
+def q_derivative_noalloc(d_in, d_out, shape, spacing, axis, forward, power, stream=0):
+    """Allocation-free constant-Q derivative of a device array (addresses as
+    ints) into a device array, asynchronous on `stream` (a cudaStream_t value;
+    0 = default stream).  For callers that cannot allocate device memory; the
+    library's fixed scratch limits the grid (see include/qvti.h)."""
+    _check(lib().qvti_q_derivative_noalloc(_V(int(d_in)), _V(int(d_out)), int(shape[0]), int(shape[1]),
+                                           int(shape[2]), float(spacing[0]), float(spacing[1]), float(spacing[2]),
+                                           int(axis), 1 if forward else 0, int(power), _V(int(stream))),
+           "qvti_q_derivative_noalloc")
 
 
 def simulation_for_case(c, vti=False, device=0):
