@@ -312,3 +312,110 @@ __device__ __forceinline__ float2 two_multiplier(float2 z, float2 zmc, float2 m1
 }
 
 }  // namespace qvti
+
+namespace qvti {
+
+// ------------------------------------------------- compile-time transforms --
+// The same Stockham sequence with the length, the radix plan, the tile width
+// and the block size known at compile time: every index division becomes a
+// shift or a multiply, every stage loop has a fixed trip count.  Used for the
+// common grid sizes; the runtime fft_run covers the rest.
+__host__ __device__ constexpr int ct_nst(int n)
+{
+    if (n == 16) return 2;
+    int m = n, s = 0;
+    const int order[7] = {16, 8, 4, 2, 3, 5, 7};
+    for (int oi = 0; oi < 7; ++oi)
+        while (m % order[oi] == 0) { m /= order[oi]; ++s; }
+    return s;
+}
+__host__ __device__ constexpr int ct_rad(int n, int stage)
+{
+    if (n == 16) return 4;
+    int m = n, s = 0;
+    const int order[7] = {16, 8, 4, 2, 3, 5, 7};
+    for (int oi = 0; oi < 7; ++oi)
+        while (m % order[oi] == 0) {
+            if (s == stage) return order[oi];
+            m /= order[oi];
+            ++s;
+        }
+    return 1;
+}
+__host__ __device__ constexpr int ct_ns(int n, int stage)
+{
+    int p = 1;
+    for (int s = 0; s < stage; ++s) p *= ct_rad(n, s);
+    return p;
+}
+
+// N points, P pencils, NT threads.  PF: element (p, i) at p + (i + pad(i)) P
+// with one extra row every 16 indices (pencil-fastest tiles, conflict-free
+// radix-16 stores); otherwise at p (N + 1) + i.
+template <int N, int P, int NT, bool PF>
+struct FftCT {
+    static constexpr int NST = ct_nst(N);
+    static constexpr int BUF = PF ? P * (N + N / 16) : P * (N + 1);  // float2 per buffer
+
+    static __device__ __forceinline__ int at(int p, int i) { return PF ? p + (i + (i >> 4)) * P : p * (N + 1) + i; }
+
+    template <int S, bool INV, class Load, class Store>
+    static __device__ __forceinline__ void stage(const float2* __restrict__ tw, float2* A, float2* B, Load& load,
+                                                 Store& store)
+    {
+        constexpr int R = ct_rad(N, S), NS = ct_ns(N, S);
+        constexpr bool FIRST = S == 0, LAST = S == NST - 1;
+        constexpr int NR = N / R, TOTAL = P * NR, TWS = N / (NS * R);
+        const float2* src = ((S - 1) & 1) ? B : A;
+        float2* dst = (S & 1) ? B : A;
+#pragma unroll
+        for (int it = 0; it < (TOTAL + NT - 1) / NT; ++it) {
+            const int t = threadIdx.x + it * NT;
+            if ((TOTAL % NT) != 0 && t >= TOTAL) break;
+            int p, j;
+            if (PF) { p = t % P; j = t / P; }
+            else    { j = t % NR; p = t / NR; }
+            const int jm = j % NS;
+            float2 v[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int idx = j + r * NR;
+                if constexpr (FIRST) v[r] = load(p, idx);
+                else v[r] = src[at(p, idx)];
+            }
+            if constexpr (!FIRST) {
+                if (jm) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        const float2 w = tw[jm * r * TWS];
+                        v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+                    }
+                }
+            }
+            Dft<R>::run(v, INV);
+            const int base = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int idx = base + r * NS;
+                if constexpr (LAST) store(p, idx, v[r]);
+                else dst[at(p, idx)] = v[r];
+            }
+        }
+        __syncthreads();
+        if constexpr (!LAST) stage<S + 1, INV>(tw, A, B, load, store);
+    }
+
+    // Stage 0 reads `load`, the last stage writes `store`; ends with
+    // __syncthreads().  Buffers: A always, B when NST > 2.
+    template <bool INV, class Load, class Store>
+    static __device__ __forceinline__ void run(const float2* __restrict__ tw, float2* A, float2* B, Load load,
+                                               Store store)
+    {
+        stage<0, INV>(tw, A, B, load, store);
+    }
+
+    // The buffer the last stage does not read.
+    static __device__ __forceinline__ float2* out_buf(float2* A, float2* B) { return ((NST - 1) & 1) ? B : A; }
+};
+
+}  // namespace qvti

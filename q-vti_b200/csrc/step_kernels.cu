@@ -23,6 +23,7 @@
 // multiplier depends on one wavenumber component, so IFFT3(M(kx) FFT3(f)) is
 // the 1D spectral derivative along x of every x line (likewise y, z).
 #include <cstdio>
+#include <type_traits>
 
 #include "engine.cuh"
 
@@ -53,6 +54,24 @@ __device__ __forceinline__ void load_table(float2* s, const float2* g, int n)
     for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
 }
 
+// A transform of the tile through the compile-time path (N > 0: length N, PC
+// pencils, NT threads) or the runtime one (N == 0: plan pl, prt pencils,
+// layout ps_rt/is_rt).  Pencil-fastest layouts carry one padding row every
+// 16 indices in both paths.
+template <int N, int PC, int NT, bool PF, bool INV, class Load, class Store>
+__device__ __forceinline__ void fft_any(const FftPlan& pl, const float2* tw, float2* A, float2* B, int prt, int ps_rt,
+                                        int is_rt, Load load, Store store)
+{
+    if constexpr (N > 0) FftCT<N, PC, NT, PF>::template run<INV>(tw, A, B, load, store);
+    else fft_run<PF>(pl, tw, A, B, prt, ps_rt, is_rt, INV, load, store, PF ? 4 : 0);
+}
+template <int N, int PC, int NT, bool PF>
+__device__ __forceinline__ float2* out_any(const FftPlan& pl, float2* A, float2* B)
+{
+    if constexpr (N > 0) return FftCT<N, PC, NT, PF>::out_buf(A, B);
+    else return fft_out_buf(pl, A, B);
+}
+
 // Derivative bookkeeping for the 9 stress-side derivatives d (G index
 // o = 3 d + j): component, axis, forward(1)/backward(0) staggered shift.
 // d: 0 dx vx, 1 dy vy, 2 dz vz (forward shift, kvx_x kvy_y kvz_z),
@@ -65,11 +84,13 @@ __constant__ int c_fwd[9] = {1, 1, 1, 0, 0, 0, 0, 0, 0};
 // ------------------------------------------------------------------ k_fz --
 // R2C along z of vx, vy, vz.  Tile: one x, P consecutive y rows (P even);
 // rows (2q, 2q+1) share one complex transform.  Output H[f][kz][x][y].
-__global__ void __launch_bounds__(kThreads) k_fz(KP k, int P)
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.nz, Qp = P / 2, ps = n + 1;
+    const int P = N > 0 ? 16 : P_rt;
+    const int n = N > 0 ? N : k.nz, Qp = P / 2, ps = n + 1;
     float2* tw = sm;
     float2* A = tw + n;
     float2* B = A + Qp * ps;
@@ -77,13 +98,13 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P)
     __syncthreads();
     const int f = blockIdx.z, x = blockIdx.y, y0 = blockIdx.x * P;
     const float* src = k.v[f];
-    float2* Z = fft_out_buf(k.pz, A, B);
+    float2* Z = out_any<N, 8, kThreads, false>(k.pz, A, B);
     auto load = [&](int q, int i) -> float2 {
         const long long b = cell(k, x, y0 + 2 * q, i);
         return make_float2(src[b], src[b + n]);
     };
     auto store = [&](int q, int i, float2 v) { Z[q * ps + i] = v; };
-    fft_run<false>(k.pz, tw, A, B, Qp, ps, 1, false, load, store);
+    fft_any<N, 8, kThreads, false, false>(k.pz, tw, A, B, Qp, ps, 1, load, store);
     float2* H = k.H[f];
     for (int t = threadIdx.x; t < k.nkz * P; t += blockDim.x) {
         const int p = t % P, kz = t / P, q = p >> 1;
@@ -101,12 +122,13 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P)
 // The field is H[0..2] (forward) or G[0..26] (inverse), by blockIdx.y.
 constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
 
-template <bool INV>
-__global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L, long long line0)
+template <int N, bool INV>
+__global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long line0)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.ny;
+    const int L = N > 0 ? 8 : L_rt;
+    const int n = N > 0 ? N : k.ny;
     float2* tw = sm;
     float2* A = tw + n;
     float2* B = A + L * (n + n / 16);
@@ -116,7 +138,7 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L, long long line0)
     float2* base = arr + (line0 + (long long)blockIdx.x * L) * n;
     auto load = [&](int p, int i) -> float2 { return base[(long long)p * n + i]; };
     auto store = [&](int p, int i, float2 v) { base[(long long)p * n + i] = v; };
-    fft_run<true>(k.py, tw, A, B, L, 1, L, INV, load, store, 4);
+    fft_any<N, 8, kCyThreads, true, INV>(k.py, tw, A, B, L, 1, L, load, store);
 }
 
 // ------------------------------------------------------------------ k_mx --
@@ -124,11 +146,13 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L, long long line0)
 // (blockIdx.z): forward x-FFT of V_c, then the 9 fields that use V_c --
 // 3 derivatives x 3 dispersion operators Ap_j D_d V_c -- each inverse
 // x-transformed on chip.  blockIdx.y + kz0 is the kz plane.
-__global__ void __launch_bounds__(kThreads) k_mx(KP k, int P, int kz0)
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.nx;
+    const int P = N > 0 ? 16 : P_rt;
+    const int n = N > 0 ? N : k.nx;
     float2* tw = sm;
     float2* tFx = tw + n;
     float2* tBx = tFx + n;
@@ -147,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P, int kz0)
         const float2* H = k.H[c];
         auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
         auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
-        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store, 4);
+        fft_any<N, 16, kThreads, true, false>(k.px, tw, A, B, P, 1, P, load, store);
     }
 
     const float kzv = k.kz[kz];
@@ -171,7 +195,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P, int kz0)
                 return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
             };
             auto store = [&](int p, int i, float2 v) { G[spec(k, kz, i, y0 + p)] = v; };
-            fft_run<true>(k.px, tw, A, B, P, 1, P, true, load, store, 4);
+            fft_any<N, 16, kThreads, true, true>(k.px, tw, A, B, P, 1, P, load, store);
         }
     }
 }
@@ -198,16 +222,19 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 // stress update; then the z derivatives of the new szz, sxz, syz for the next
 // velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
 // z terms, and the source injection.
-__global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
+template <int N>
+__global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.nz, Qp = P / 2, np1 = n + 1, nx = k.nx, ny = k.ny, pml = k.pml;
-    const int two_buf = k.pz.nst > 2;
+    const int P = N > 0 ? 4 : P_rt;
+    const int n = N > 0 ? N : k.nz, Qp = P / 2, np1 = n + 1, nx = k.nx, ny = k.ny, pml = k.pml;
+    const int two_buf = N > 0 ? (ct_nst(N) > 2) : (k.pz.nst > 2);
+    const int bufA = 9 * Qp * (n + n / 16);
     float2* tw = sm;
     float2* A = tw + n;
-    float2* B = A + 9 * Qp * n;  // aliases S when the transform has two stages
-    float* S = reinterpret_cast<float*>(B + (two_buf ? 9 * Qp * n : 0));  // [9][P][np1]
+    float2* B = A + bufA;  // aliases S when the transform has two stages
+    float* S = reinterpret_cast<float*>(B + (two_buf ? bufA : 0));  // [9][P][np1]
     float* D = S + 9 * P * np1;                                           // [3][P][np1]: szz sxz syz
     load_table(tw, k.tw_z, n);
     __syncthreads();
@@ -268,7 +295,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
             S[(f * P + 2 * q) * np1 + i] = v.x;
             S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_run<true>(k.pz, tw, A, B, npen, 1, npen, true, load, store);
+        if (grp == 0) fft_any<N, 18, kThreads, true, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        else fft_any<N, 12, kThreads, true, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
 
         // 2. stress update of the group.  Each thread owns kCells cells; all
         //    their streaming inputs are loaded before any store so the loads
@@ -334,38 +362,45 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
                         const float q13z = QL(a13, Z0, Z1), q33z = QL(a33, Z0, Z1);
 #undef QD
 #undef QL
+                        // C-PML terms of the slabs this cell is in: every load is
+                        // issued before any store (the arrays are distinct, but
+                        // through the parameter struct the compiler cannot know)
+                        const bool sx = in_slab(x, nx, pml), sy = in_slab(y, ny, pml), sz = in_slab(z, n, pml);
+                        float qo[8], po[8];
+#pragma unroll
+                        for (int m = 0; m < 8; ++m) {
+                            const bool on = m < 3 ? sx : (m < 6 ? sy : sz);
+                            qo[m] = on ? k.qn[m][ip] : 0.f;
+                            po[m] = on ? k.phn[m][ip] : 0.f;
+                        }
                         // loss: sum_terms tau-coefficient x (S - S_prev)/dt = (Q - Q_prev)/dt
                         const float Qxx = q11x + q12y + q13z, Qyy = q12x + q11y + q13z, Qzz = q13x + q13y + q33z;
                         const float Lxx = (Qxx - in[u][3]) * inv_dt;
                         const float Lyy = (Qyy - in[u][4]) * inv_dt;
                         const float Lzz = (Qzz - in[u][5]) * inv_dt;
+                        const float dterm[8] = {d11x, d12x, d13x, d12y, d11y, d13y, d13z, d33z};
+                        const float qterm[8] = {q11x, q12x, q13x, q12y, q11y, q13y, q13z, q33z};
+                        float ph[8];
+#pragma unroll
+                        for (int m = 0; m < 8; ++m) {
+                            const float a = m < 3 ? k.ax[x] : (m < 6 ? k.ay[y] : k.az[z]);
+                            const float b = m < 3 ? k.bx[x] : (m < 6 ? k.by[y] : k.bz[z]);
+                            const float T = dterm[m] + (qterm[m] - qo[m]) * inv_dt;
+                            ph[m] = po[m] + dt * (-a * po[m] - b * T);
+                        }
+                        if (!sx) { ph[0] = ph[1] = ph[2] = 0.f; }
+                        if (!sy) { ph[3] = ph[4] = ph[5] = 0.f; }
+                        if (!sz) { ph[6] = ph[7] = 0.f; }
+                        // ph[6] is phi_vz_zx == phi_vz_zy
+                        sxx = sxx + dt * (d11x + d12y + d13z + Lxx + ph[0] + ph[3] + ph[6]);
+                        syy = syy + dt * (d12x + d11y + d13z + Lyy + ph[1] + ph[4] + ph[6]);
+                        szz = szz + dt * (d13x + d13y + d33z + Lzz + ph[2] + ph[5] + ph[7]);
                         q0[ip] = Qxx; q1[ip] = Qyy; q2[ip] = Qzz;
-                        float pxx = 0.f, pxy = 0.f, pxz = 0.f, pyx = 0.f, pyy = 0.f, pyz = 0.f, pzxy = 0.f, pzz = 0.f;
-                        auto mem = [&](int m, float dterm, float qterm, float a, float b) {
-                            const float T = dterm + (qterm - k.qn[m][ip]) * inv_dt;
-                            k.qn[m][ip] = qterm;
-                            float ph = k.phn[m][ip];
-                            ph = ph + dt * (-a * ph - b * T);
-                            k.phn[m][ip] = ph;
-                            return ph;
-                        };
-                        if (in_slab(x, nx, pml)) {
-                            pxx = mem(0, d11x, q11x, k.ax[x], k.bx[x]);
-                            pxy = mem(1, d12x, q12x, k.ax[x], k.bx[x]);
-                            pxz = mem(2, d13x, q13x, k.ax[x], k.bx[x]);
+#pragma unroll
+                        for (int m = 0; m < 8; ++m) {
+                            const bool on = m < 3 ? sx : (m < 6 ? sy : sz);
+                            if (on) { k.qn[m][ip] = qterm[m]; k.phn[m][ip] = ph[m]; }
                         }
-                        if (in_slab(y, ny, pml)) {
-                            pyx = mem(3, d12y, q12y, k.ay[y], k.by[y]);
-                            pyy = mem(4, d11y, q11y, k.ay[y], k.by[y]);
-                            pyz = mem(5, d13y, q13y, k.ay[y], k.by[y]);
-                        }
-                        if (in_slab(z, n, pml)) {
-                            pzxy = mem(6, d13z, q13z, k.az[z], k.bz[z]);  // phi_vz_zx == phi_vz_zy
-                            pzz = mem(7, d33z, q33z, k.az[z], k.bz[z]);
-                        }
-                        sxx = sxx + dt * (d11x + d12y + d13z + Lxx + pxx + pyx + pzxy);
-                        syy = syy + dt * (d12x + d11y + d13z + Lyy + pxy + pyy + pzxy);
-                        szz = szz + dt * (d13x + d13y + d33z + Lzz + pxz + pyz + pzz);
                     }
                     if (ip == src_ip && it < k.nt_rec) {  // cu:772-777, after the update
                         if (k.src_type == 1) {
@@ -415,31 +450,23 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
                         const float dB = mu[0] * B0 + mu[1] * B1 + mu[2] * B2, qB = mu[3] * B0 + mu[4] * B1;
                         const float Qs = qA + qB;
                         const float L = (Qs - in[u][1]) * inv_dt;
-                        qg[ip] = Qs;
                         // term A: xz vx_z (z slab), xy vx_y (y slab), yz vy_z (z slab)
                         // term B: xz vz_x (x slab), xy vy_x (x slab), yz vz_y (y slab)
                         const int mA = (grp - 1) * 2, mB = mA + 1;
-                        auto mem = [&](int m, float dterm, float qterm, float a, float b) {
-                            const float T = dterm + (qterm - k.qs[m][ip]) * inv_dt;
-                            k.qs[m][ip] = qterm;
-                            float ph = k.phs[m][ip];
-                            ph = ph + dt * (-a * ph - b * T);
-                            k.phs[m][ip] = ph;
-                            return ph;
-                        };
-                        float phA = 0.f, phB = 0.f;
-                        if (grp == 1) {
-                            if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
-                            if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
-                        } else if (grp == 2) {
-                            if (in_slab(y, ny, pml)) phA = mem(mA, dA, qA, k.ayh[y], k.byh[y]);
-                            if (in_slab(x, nx, pml)) phB = mem(mB, dB, qB, k.axh[x], k.bxh[x]);
-                        } else {
-                            if (in_slab(z, n, pml)) phA = mem(mA, dA, qA, k.azh[z], k.bzh[z]);
-                            if (in_slab(y, ny, pml)) phB = mem(mB, dB, qB, k.ayh[y], k.byh[y]);
-                        }
+                        const bool onA = grp == 2 ? in_slab(y, ny, pml) : in_slab(z, n, pml);
+                        const bool onB = grp == 3 ? in_slab(y, ny, pml) : in_slab(x, nx, pml);
+                        const float qoA = onA ? k.qs[mA][ip] : 0.f, poA = onA ? k.phs[mA][ip] : 0.f;
+                        const float qoB = onB ? k.qs[mB][ip] : 0.f, poB = onB ? k.phs[mB][ip] : 0.f;
+                        const float aA = grp == 2 ? k.ayh[y] : k.azh[z], bA = grp == 2 ? k.byh[y] : k.bzh[z];
+                        const float aB = grp == 3 ? k.ayh[y] : k.axh[x], bB = grp == 3 ? k.byh[y] : k.bxh[x];
+                        const float TA = dA + (qA - qoA) * inv_dt, TB = dB + (qB - qoB) * inv_dt;
+                        const float phA = onA ? poA + dt * (-aA * poA - bA * TA) : 0.f;
+                        const float phB = onB ? poB + dt * (-aB * poB - bB * TB) : 0.f;
                         sig = sig + dt * (dA + phA + dB + phB + L);
+                        qg[ip] = Qs;
                         sg[ip] = sig;
+                        if (onA) { k.qs[mA][ip] = qA; k.phs[mA][ip] = phA; }
+                        if (onB) { k.qs[mB][ip] = qB; k.phs[mB][ip] = phB; }
                     }
                     if (grp == 1) D[(1 * P + p) * np1 + z] = sig;
                     if (grp == 3) D[(2 * P + p) * np1 + z] = sig;
@@ -458,49 +485,56 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P)
             const int f = pp / Qp, q = pp - f * Qp;
             return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
         };
-        float2* Zf = fft_out_buf(k.pz, A, B);
+        float2* Zf = out_any<N, 6, kThreads, false>(k.pz, A, B);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
-        fft_run<false>(k.pz, tw, A, B, npen, np1, 1, false, load, store_f);
+        fft_any<N, 6, kThreads, false, false>(k.pz, tw, A, B, npen, np1, 1, load, store_f);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
             return cmul(Zf[pp * np1 + i], cscale(f == 0 ? k.Bz[i] : k.Fz[i], inv_n));
         };
+        // derivatives parked in D (its stresses were consumed by stage 0 of
+        // the forward transform), then written out with all loads first
         auto store_i = [&](int pp, int i, float2 v) {
             const int f = pp / Qp, q = pp - f * Qp;
-            const int rc = f == 0 ? 2 : f == 1 ? 0 : 1;
-            const int phm = f == 0 ? 8 : f == 1 ? 2 : 5;  // php: pzz_z, pxz_z, pyz_z
-            const bool zin = i < n - 1 && x < nx - 1;
-            const bool zslab = in_slab(i, n, pml);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int y = y0 + 2 * q + h;
-                const long long ip = cell(k, x, y, i);
-                const float part = h ? v.y : v.x;
-                float r = part;
-                if (zslab && zin && y < ny - 1) {
-                    float ph = k.php[phm][ip];
-                    const float a = f == 0 ? k.azh[i] : k.az[i];
-                    const float b = f == 0 ? k.bzh[i] : k.bz[i];
-                    ph = ph + dt * (-a * ph - b * part);
-                    k.php[phm][ip] = ph;
-                    r += ph;
-                }
-                k.R[rc][ip] = r;
-            }
+            D[(f * P + 2 * q) * np1 + i] = v.x;
+            D[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_run<false>(k.pz, tw, X1, Zf, npen, np1, 1, true, load_i, store_i);
+        fft_any<N, 6, kThreads, false, true>(k.pz, tw, X1, Zf, npen, np1, 1, load_i, store_i);
+        for (int t = threadIdx.x; t < 3 * P * n; t += blockDim.x) {
+            const int i = t % n, fp = t / n, f = fp / P, p = fp - f * P;
+            const int y = y0 + p;
+            const int rc = f == 0 ? 2 : f == 1 ? 0 : 1;
+            float* __restrict__ ph = k.php[f == 0 ? 8 : f == 1 ? 2 : 5];  // pzz_z, pxz_z, pyz_z
+            const long long ip = cell(k, x, y, i);
+            const bool slab = in_slab(i, n, pml) && i < n - 1 && x < nx - 1 && y < ny - 1;
+            const float old = slab ? ph[ip] : 0.f;
+            const float part = D[(f * P + p) * np1 + i];
+            float r = part;
+            if (slab) {
+                const float a = f == 0 ? k.azh[i] : k.az[i];
+                const float b = f == 0 ? k.bzh[i] : k.bz[i];
+                const float nw = old + dt * (-a * old - b * part);
+                ph[ip] = nw;
+                r += nw;
+            }
+            k.R[rc][ip] = r;
+        }
     }
 }
 
 // ------------------------------------------------------------------ k_vy --
 // y-derivatives of sxy (+, -> vx), syy (-, -> vy), syz (+, -> vz) for one x
-// and P consecutive z; C-PML y terms; accumulate into R.
-__global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
+// and P consecutive z; C-PML y terms; accumulate into R.  Each pass parks its
+// derivatives in shared memory; the epilogue then loads everything a cell
+// needs before storing anything (no store can delay a later load).
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 {
+    const int P = N > 0 ? 16 : P_rt;
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.ny, ny = k.ny, pml = k.pml;
+    const int n = N > 0 ? N : k.ny, ny = n, pml = k.pml;
     float2* tw = sm;
     float2* tF = tw + n;
     float2* tB = tF + n;
@@ -514,83 +548,105 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P)
     const int x = blockIdx.y, z0 = blockIdx.x * P;
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool xin = x < k.nx - 1;
-    const float* sxy = k.s[3];
-    const float* syy = k.s[1];
-    const float* syz = k.s[5];
+    const float* __restrict__ sxy = k.s[3];
+    const float* __restrict__ syy = k.s[1];
+    const float* __restrict__ syz = k.s[5];
+    float* __restrict__ R0 = k.R[0];
+    float* __restrict__ R1 = k.R[1];
+    float* __restrict__ R2 = k.R[2];
+    float* __restrict__ f1 = k.php[1];  // phi_pxy_y, b_y
+    float* __restrict__ f4 = k.php[4];  // phi_pyy_y, averaged b_y
+    float* __restrict__ f7 = k.php[7];  // phi_pyz_y, b_y
 
-    // pass 1: sxy + i syy
+    // pass 1: sxy + i syy -> dy+ sxy (vx), dy- syy (vy)
     {
-        float2* Zf = fft_out_buf(k.py, A, B);
+        float2* Zf = out_any<N, 16, kThreads, true>(k.py, A, B);
         auto load = [&](int p, int i) -> float2 {
             const long long ip = cell(k, x, i, z0 + p);
             return make_float2(sxy[ip], syy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_run<true>(k.py, tw, A, B, P, 1, P, false, load, store, 4);
+        fft_any<N, 16, kThreads, true, false>(k.py, tw, A, B, P, 1, P, load, store);
         float2* X1 = Zf == A ? B : A;
+        // [2][n][P] in the buffer the last stage does not read
+        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, true>(k.py, X1, Zf));
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
             return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tF[i], inv_n), cscale(tB[i], inv_n));
         };
         auto store_i = [&](int p, int i, float2 v) {
-            const int z = z0 + p;
-            const long long ip = cell(k, x, i, z);
-            float rx = v.x, ry = v.y;
-            if (in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1) {
-                float ph = k.php[1][ip];  // phi_pxy_y, b_y
-                ph = ph + dt * (-k.ay[i] * ph - k.by[i] * v.x);
-                k.php[1][ip] = ph;
-                rx += ph;
-                float qh = k.php[4][ip];  // phi_pyy_y, averaged b_y
-                qh = qh + dt * (-k.ayh[i] * qh - k.byh[i] * v.y);
-                k.php[4][ip] = qh;
-                ry += qh;
-            }
-            k.R[0][ip] += rx;
-            k.R[1][ip] += ry;
+            D[i * P + p] = v.x;
+            D[(n + i) * P + p] = v.y;
         };
-        fft_run<true>(k.py, tw, X1, Zf, P, 1, P, true, load_i, store_i, 4);
+        fft_any<N, 16, kThreads, true, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
+        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
+            const int p = t % P, i = t / P, z = z0 + p;
+            const long long ip = cell(k, x, i, z);
+            const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
+            const float r0 = R0[ip], r1 = R1[ip];
+            const float p1 = slab ? f1[ip] : 0.f, p4 = slab ? f4[ip] : 0.f;
+            const float dx = D[i * P + p], dy = D[(n + i) * P + p];
+            float rx = r0 + dx, ry = r1 + dy;
+            if (slab) {
+                const float q1 = p1 + dt * (-k.ay[i] * p1 - k.by[i] * dx);
+                const float q4 = p4 + dt * (-k.ayh[i] * p4 - k.byh[i] * dy);
+                rx += q1;
+                ry += q4;
+                f1[ip] = q1;
+                f4[ip] = q4;
+            }
+            R0[ip] = rx;
+            R1[ip] = ry;
+        }
+        __syncthreads();
     }
-    // pass 2: syz, pencils (2q, 2q+1)
+    // pass 2: syz, pencils (2q, 2q+1) -> dy+ syz (vz)
     {
         const int Qp = P / 2;
-        float2* Zf = fft_out_buf(k.py, A, B);
+        float2* Zf = out_any<N, 8, kThreads, true>(k.py, A, B);
         auto load = [&](int q, int i) -> float2 {
             const long long ip = cell(k, x, i, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(syz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_run<true>(k.py, tw, A, B, Qp, 1, Qp, false, load, store, 4);
+        fft_any<N, 8, kThreads, true, false>(k.py, tw, A, B, Qp, 1, Qp, load, store);
         float2* X1 = Zf == A ? B : A;
+        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, true>(k.py, X1, Zf));  // [n][P]
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int z = z0 + 2 * q + h;
-                const long long ip = cell(k, x, i, z);
-                const float part = h ? v.y : v.x;
-                float r = part;
-                if (in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1) {
-                    float ph = k.php[7][ip];  // phi_pyz_y, b_y
-                    ph = ph + dt * (-k.ay[i] * ph - k.by[i] * part);
-                    k.php[7][ip] = ph;
-                    r += ph;
-                }
-                k.R[2][ip] += r;
-            }
+            D[i * P + 2 * q] = v.x;
+            D[i * P + 2 * q + 1] = v.y;
         };
-        fft_run<true>(k.py, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i, 4);
+        fft_any<N, 8, kThreads, true, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
+        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
+            const int p = t % P, i = t / P, z = z0 + p;
+            const long long ip = cell(k, x, i, z);
+            const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
+            const float r2 = R2[ip];
+            const float p7 = slab ? f7[ip] : 0.f;
+            const float dz = D[i * P + p];
+            float rz = r2 + dz;
+            if (slab) {
+                const float q7 = p7 + dt * (-k.ay[i] * p7 - k.by[i] * dz);
+                rz += q7;
+                f7[ip] = q7;
+            }
+            R2[ip] = rz;
+        }
     }
 }
 
 // ------------------------------------------------------------------ k_vx --
 // x-derivatives of sxx (-, vx), sxy (+, vy), sxz (+, vz); C-PML x terms and
-// the velocity update (cuda_kernel_calculate_v, cu:1018-1101).
-__global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
+// the velocity update (cuda_kernel_calculate_v, cu:1018-1101); same
+// park-then-epilogue structure as k_vy.
+template <int N>
+__global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
 {
+    const int P = N > 0 ? 16 : P_rt;
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int n = k.nx, nx = k.nx, pml = k.pml;
+    const int n = N > 0 ? N : k.nx, nx = n, pml = k.pml;
     float2* tw = sm;
     float2* tF = tw + n;
     float2* tB = tF + n;
@@ -603,74 +659,96 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P)
     const int y = blockIdx.y, z0 = blockIdx.x * P;
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool yin = y < k.ny - 1;
-    const float* sxx = k.s[0];
-    const float* sxy = k.s[3];
-    const float* sxz = k.s[4];
+    const float* __restrict__ sxx = k.s[0];
+    const float* __restrict__ sxy = k.s[3];
+    const float* __restrict__ sxz = k.s[4];
+    float* __restrict__ v0 = k.v[0];
+    float* __restrict__ v1 = k.v[1];
+    float* __restrict__ v2 = k.v[2];
+    const float* __restrict__ R0 = k.R[0];
+    const float* __restrict__ R1 = k.R[1];
+    const float* __restrict__ R2 = k.R[2];
+    const float* __restrict__ ri0 = k.rinv[0];
+    const float* __restrict__ ri1 = k.rinv[1];
+    const float* __restrict__ ri2 = k.rinv[2];
+    float* __restrict__ f0 = k.php[0];  // phi_pxx_x, averaged b_x
+    float* __restrict__ f3 = k.php[3];  // phi_pxy_x, b_x
+    float* __restrict__ f6 = k.php[6];  // phi_pxz_x, b_x
 
-    // pass 1: sxx + i sxy -> vx, vy
+    // pass 1: sxx + i sxy -> dx- sxx (vx), dx+ sxy (vy)
     {
-        float2* Zf = fft_out_buf(k.px, A, B);
+        float2* Zf = out_any<N, 16, kThreads, true>(k.px, A, B);
         auto load = [&](int p, int i) -> float2 {
             const long long ip = cell(k, i, y, z0 + p);
             return make_float2(sxx[ip], sxy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store, 4);
+        fft_any<N, 16, kThreads, true, false>(k.px, tw, A, B, P, 1, P, load, store);
         float2* X1 = Zf == A ? B : A;
+        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, true>(k.px, X1, Zf));  // [2][n][P]
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
             return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tB[i], inv_n), cscale(tF[i], inv_n));
         };
         auto store_i = [&](int p, int i, float2 v) {
-            const int z = z0 + p;
-            if (!(i < nx - 1 && yin && z < k.nz - 1)) return;
-            const long long ip = cell(k, i, y, z);
-            float px = v.x, py = v.y;
-            if (in_slab(i, nx, pml)) {
-                float ph = k.php[0][ip];  // phi_pxx_x, averaged b_x
-                ph = ph + dt * (-k.axh[i] * ph - k.bxh[i] * v.x);
-                k.php[0][ip] = ph;
-                px += ph;
-                float qh = k.php[3][ip];  // phi_pxy_x, b_x
-                qh = qh + dt * (-k.ax[i] * qh - k.bx[i] * v.y);
-                k.php[3][ip] = qh;
-                py += qh;
-            }
-            k.v[0][ip] += dt * k.rinv[0][ip] * (px + k.R[0][ip]);
-            k.v[1][ip] += dt * k.rinv[1][ip] * (py + k.R[1][ip]);
+            D[i * P + p] = v.x;
+            D[(n + i) * P + p] = v.y;
         };
-        fft_run<true>(k.px, tw, X1, Zf, P, 1, P, true, load_i, store_i, 4);
+        fft_any<N, 16, kThreads, true, true>(k.px, tw, X1, Zf, P, 1, P, load_i, store_i);
+        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
+            const int p = t % P, i = t / P, z = z0 + p;
+            if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
+            const long long ip = cell(k, i, y, z);
+            const bool slab = in_slab(i, nx, pml);
+            const float a0 = v0[ip], a1 = v1[ip], r0 = R0[ip], r1 = R1[ip], w0 = ri0[ip], w1 = ri1[ip];
+            const float p0 = slab ? f0[ip] : 0.f, p3 = slab ? f3[ip] : 0.f;
+            float px = D[i * P + p], py = D[(n + i) * P + p];
+            if (slab) {
+                const float q0 = p0 + dt * (-k.axh[i] * p0 - k.bxh[i] * px);
+                const float q3 = p3 + dt * (-k.ax[i] * p3 - k.bx[i] * py);
+                px += q0;
+                py += q3;
+                f0[ip] = q0;
+                f3[ip] = q3;
+            }
+            v0[ip] = a0 + dt * w0 * (px + r0);
+            v1[ip] = a1 + dt * w1 * (py + r1);
+        }
+        __syncthreads();
     }
-    // pass 2: sxz pencils (2q, 2q+1) -> vz
+    // pass 2: sxz pencils (2q, 2q+1) -> dx+ sxz (vz)
     {
         const int Qp = P / 2;
-        float2* Zf = fft_out_buf(k.px, A, B);
+        float2* Zf = out_any<N, 8, kThreads, true>(k.px, A, B);
         auto load = [&](int q, int i) -> float2 {
             const long long ip = cell(k, i, y, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_run<true>(k.px, tw, A, B, Qp, 1, Qp, false, load, store, 4);
+        fft_any<N, 8, kThreads, true, false>(k.px, tw, A, B, Qp, 1, Qp, load, store);
         float2* X1 = Zf == A ? B : A;
+        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, true>(k.px, X1, Zf));  // [n][P]
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
-            if (!(i < nx - 1 && yin)) return;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int z = z0 + 2 * q + h;
-                if (z >= k.nz - 1) continue;
-                const long long ip = cell(k, i, y, z);
-                float part = h ? v.y : v.x;
-                if (in_slab(i, nx, pml)) {
-                    float ph = k.php[6][ip];  // phi_pxz_x, b_x
-                    ph = ph + dt * (-k.ax[i] * ph - k.bx[i] * part);
-                    k.php[6][ip] = ph;
-                    part += ph;
-                }
-                k.v[2][ip] += dt * k.rinv[2][ip] * (part + k.R[2][ip]);
-            }
+            D[i * P + 2 * q] = v.x;
+            D[i * P + 2 * q + 1] = v.y;
         };
-        fft_run<true>(k.px, tw, X1, Zf, Qp, 1, Qp, true, load_i, store_i, 4);
+        fft_any<N, 8, kThreads, true, true>(k.px, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
+        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
+            const int p = t % P, i = t / P, z = z0 + p;
+            if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
+            const long long ip = cell(k, i, y, z);
+            const bool slab = in_slab(i, nx, pml);
+            const float a2 = v2[ip], r2 = R2[ip], w2 = ri2[ip];
+            const float p6 = slab ? f6[ip] : 0.f;
+            float pz = D[i * P + p];
+            if (slab) {
+                const float q6 = p6 + dt * (-k.ax[i] * p6 - k.bx[i] * pz);
+                pz += q6;
+                f6[ip] = q6;
+            }
+            v2[ip] = a2 + dt * w2 * (pz + r2);
+        }
     }
 }
 
@@ -825,14 +903,14 @@ __global__ void __launch_bounds__(kThreads) kq_mx(KP k, int P, int axis, int fwd
     float2* tw = sm;
     float2* V = tw + n;   // [n][P]
     float2* A = V + n * P;
-    float2* B = A + n * P;
+    float2* B = A + (n + n / 16) * P;
     load_table(tw, k.tw_x, n);
     __syncthreads();
     const int kz = blockIdx.y, y0 = blockIdx.x * P;
     float2* H = k.H[0];
     auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
     auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
-    fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store);
+    fft_run<true>(k.px, tw, A, B, P, 1, P, false, load, store, 4);
     const float kz2 = k.kz[kz] * k.kz[kz];
     auto load_i = [&](int p, int i) -> float2 {
         const float kyv = k.ky[y0 + p], kxv = k.kx[i];
@@ -845,7 +923,7 @@ __global__ void __launch_bounds__(kThreads) kq_mx(KP k, int P, int axis, int fwd
         return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
     };
     auto store_i = [&](int p, int i, float2 v) { H[spec(k, kz, i, y0 + p)] = v; };
-    fft_run<true>(k.px, tw, A, B, P, 1, P, true, load_i, store_i);
+    fft_run<true>(k.px, tw, A, B, P, 1, P, true, load_i, store_i, 4);
 }
 
 __global__ void __launch_bounds__(kThreads) kq_iz(KP k, int P, float* out)
@@ -855,7 +933,7 @@ __global__ void __launch_bounds__(kThreads) kq_iz(KP k, int P, float* out)
     const int n = k.nz, Qp = P / 2;
     float2* tw = sm;
     float2* A = tw + n;
-    float2* B = A + Qp * n;
+    float2* B = A + Qp * (n + n / 16);
     load_table(tw, k.tw_z, n);
     __syncthreads();
     const int x = blockIdx.y, y0 = blockIdx.x * P;
@@ -872,7 +950,7 @@ __global__ void __launch_bounds__(kThreads) kq_iz(KP k, int P, float* out)
         out[cell(k, x, y0 + 2 * q, i)] = v.x;
         out[cell(k, x, y0 + 2 * q + 1, i)] = v.y;
     };
-    fft_run<true>(k.pz, tw, A, B, Qp, 1, Qp, true, load, store);
+    fft_run<true>(k.pz, tw, A, B, Qp, 1, Qp, true, load, store, 4);
 }
 
 // --------------------------------------------------------- tile selection --
@@ -894,7 +972,7 @@ size_t smem_mx(const KP& k, int P)
 // S[9][P][nz+1] | D[3][P][nz+1].
 size_t smem_sigma(const KP& k, int P)
 {
-    const size_t bufA = (size_t)9 * (P / 2) * k.nz;
+    const size_t bufA = (size_t)9 * (P / 2) * (k.nz + k.nz / 16);
     const int nb = k.pz.nst > 2 ? 2 : 1;
     return sizeof(float2) * (k.nz + nb * bufA) + sizeof(float) * (size_t)12 * P * (k.nz + 1);
 }
@@ -902,6 +980,24 @@ size_t smem_sigma(const KP& k, int P)
 size_t smem_vyx(int n, int P) { return sizeof(float2) * (3 * n + 2 * (n + n / 16) * P); }
 
 }  // namespace
+
+// Lengths with a compile-time transform path (grids whose three dimensions
+// are multiples of 16); any other even 2/3/5/7-smooth size takes the runtime
+// path.
+template <class F>
+void dispatch_len(int n, F&& f)
+{
+    switch (n) {
+        case 64: f(std::integral_constant<int, 64>{}); break;
+        case 96: f(std::integral_constant<int, 96>{}); break;
+        case 128: f(std::integral_constant<int, 128>{}); break;
+        case 256: f(std::integral_constant<int, 256>{}); break;
+        case 512: f(std::integral_constant<int, 512>{}); break;
+        default: f(std::integral_constant<int, 0>{}); break;
+    }
+}
+
+bool ct_grid(const KP& k) { return k.nx % 16 == 0 && k.ny % 16 == 0 && k.nz % 16 == 0; }
 
 int configure_kernels()
 {
@@ -911,13 +1007,17 @@ int configure_kernels()
         cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         if (r != cudaSuccess) e = r;
     };
-    set((const void*)k_fz);
-    set((const void*)k_cy<false>);
-    set((const void*)k_cy<true>);
-    set((const void*)k_mx);
-    set((const void*)k_sigma);
-    set((const void*)k_vy);
-    set((const void*)k_vx);
+    for (int n : {0, 64, 96, 128, 256, 512})
+        dispatch_len(n, [&](auto NN) {
+            constexpr int N = decltype(NN)::value;
+            set((const void*)k_fz<N>);
+            set((const void*)k_cy<N, false>);
+            set((const void*)k_cy<N, true>);
+            set((const void*)k_mx<N>);
+            set((const void*)k_sigma<N>);
+            set((const void*)k_vy<N>);
+            set((const void*)k_vx<N>);
+        });
     set((const void*)k_deriv1d);
     set((const void*)kq_mx);
     set((const void*)kq_iz);
@@ -937,33 +1037,48 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
             prof->kind[prof->n++] = kind;
         }
     };
+    const bool ct = ct_grid(k);
+    auto len = [&](int n) { return ct ? n : 0; };
     mark(-1);
     const int Pv = tile_of(k.nz, 16);
-    k_vy<<<dim3(k.nz / Pv, k.nx), kThreads, smem_vyx(k.ny, Pv), st>>>(k, Pv);
+    dispatch_len(len(k.ny), [&](auto NN) {
+        k_vy<decltype(NN)::value><<<dim3(k.nz / Pv, k.nx), kThreads, smem_vyx(k.ny, Pv), st>>>(k, Pv);
+    });
     mark(0);
-    k_vx<<<dim3(k.nz / Pv, k.ny), kThreads, smem_vyx(k.nx, Pv), st>>>(k, Pv);
+    dispatch_len(len(k.nx), [&](auto NN) {
+        k_vx<decltype(NN)::value><<<dim3(k.nz / Pv, k.ny), kThreads, smem_vyx(k.nx, Pv), st>>>(k, Pv);
+    });
     mark(1);
     const int Pz = tile_of(k.ny, 16);
-    k_fz<<<dim3(k.ny / Pz, k.nx, 3), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
+    dispatch_len(len(k.nz), [&](auto NN) {
+        k_fz<decltype(NN)::value><<<dim3(k.ny / Pz, k.nx, 3), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
+    });
     mark(2);
-    // k-space passes in batches of kz planes: the 27 spectra a batch's k_mx
-    // writes are read back by its k_cy<true> while still in L2 (a batch is
-    // sized to ~48 MB of spectra), so they reach HBM once instead of twice.
+    // k-space passes, optionally in batches of kz planes (KP::kz_batch).
     const int L = tile_of(k.nx, 8);
     const int Pm = tile_of(k.ny, 16);
     const int batch = k.kz_batch > 0 ? k.kz_batch : k.nkz;
     for (int kz0 = 0; kz0 < k.nkz; kz0 += batch) {
         const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
         const long long line0 = (long long)kz0 * k.nx;
-        k_cy<false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+        dispatch_len(len(k.ny), [&](auto NN) {
+            k_cy<decltype(NN)::value, false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+        });
         mark(3);
-        k_mx<<<dim3(k.ny / Pm, nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
+        dispatch_len(len(k.nx), [&](auto NN) {
+            k_mx<decltype(NN)::value><<<dim3(k.ny / Pm, nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
+        });
         mark(4);
-        k_cy<true><<<dim3(nb * k.nx / L, kNumG), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+        dispatch_len(len(k.ny), [&](auto NN) {
+            k_cy<decltype(NN)::value, true><<<dim3(nb * k.nx / L, kNumG), kCyThreads, smem_cy(k, L), st>>>(k, L,
+                                                                                                           line0);
+        });
         mark(5);
     }
     const int Ps = tile_of(k.ny, 4);
-    k_sigma<<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
+    dispatch_len(len(k.nz), [&](auto NN) {
+        k_sigma<decltype(NN)::value><<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
+    });
     mark(6);
     if (k.rn > 0) {
         k_rec<<<(k.rn + 255) / 256, 256, 0, st>>>(k);
@@ -991,14 +1106,16 @@ void launch_mu_rinv(const KP& k, const float* rho, const float* const* sset, cud
 void launch_q_derivative(const KP& k, int axis, int fwd, int pw, float* out, cudaStream_t st)
 {
     const int Pz = tile_of(k.ny, 16);
-    k_fz<<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
+    k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
     const int L = tile_of(k.nx, 8);
-    k_cy<false><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    k_cy<0, false><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
     const int Pm = tile_of(k.ny, 8);
-    kq_mx<<<dim3(k.ny / Pm, k.nkz), kThreads, sizeof(float2) * (k.nx + 3 * k.nx * Pm), st>>>(k, Pm, axis, fwd, pw);
-    k_cy<true><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    kq_mx<<<dim3(k.ny / Pm, k.nkz), kThreads, sizeof(float2) * (k.nx + k.nx * Pm + 2 * (k.nx + k.nx / 16) * Pm), st>>>(
+        k, Pm, axis, fwd, pw);
+    k_cy<0, true><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
     const int Pi = tile_of(k.ny, 8);
-    kq_iz<<<dim3(k.ny / Pi, k.nx), kThreads, sizeof(float2) * (k.nz + 2 * (Pi / 2) * k.nz), st>>>(k, Pi, out);
+    kq_iz<<<dim3(k.ny / Pi, k.nx), kThreads, sizeof(float2) * (k.nz + 2 * (Pi / 2) * (k.nz + k.nz / 16)), st>>>(k, Pi,
+                                                                                                               out);
 }
 
 void launch_derivative_1d(const KP& k, int axis, int fwd, const float* in, float* out, cudaStream_t st)

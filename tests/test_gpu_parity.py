@@ -94,3 +94,18 @@ def test_explosive_source_against_oracle(qvti, oracle):
     ours = qvti.run_case(c, snaps=[40], src_type=qvti.SRC_EXPLOSIVE, ref_offset=False)
     ref = oracle.run_case(c, snaps=[40], src_type=1, ref_offset=False)
     _compare(ours, ref, "explosive")
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (64, 128, 96)])
+def test_compile_time_path_against_oracle(qvti, oracle, n):
+    """Grids whose dimensions are multiples of 16 with a compiled transform
+    length take the compile-time FFT path; VTI, heterogeneous, 100 steps,
+    receivers 6 cells above the source so the direct wave is recorded."""
+    c = qc.heterogeneous_case(n=n, pml=10, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=100, f0=30.0, seed=21,
+                              src=(n[0] // 2, n[1] // 2, n[2] // 2), r_iz=n[2] // 2 - 6, name="ct")
+    rng = np.random.default_rng(4)
+    c["eps"] = (0.05 + 0.2 * rng.random(c["velp"].shape)).astype(np.float32)
+    c["delta"] = (0.12 * rng.random(c["velp"].shape)).astype(np.float32)
+    ours = qvti.run_case(c, snaps=[100], vti=True)
+    ref = oracle.run_case(c, snaps=[100], vti=True)
+    _compare(ours, ref, "ct%dx%dx%d" % n)
