@@ -349,15 +349,30 @@ __host__ __device__ constexpr int ct_ns(int n, int stage)
     return p;
 }
 
-// N points, P pencils, NT threads.  PF: element (p, i) at p + (i + pad(i)) P
-// with one extra row every 16 indices (pencil-fastest tiles, conflict-free
-// radix-16 stores); otherwise at p (N + 1) + i.
-template <int N, int P, int NT, bool PF>
-struct FftCT {
-    static constexpr int NST = ct_nst(N);
-    static constexpr int BUF = PF ? P * (N + N / 16) : P * (N + 1);  // float2 per buffer
+// Tile layouts in shared memory (element (p, i) of pencil p, index i):
+//   kLine     p (N + 1) + i                  line-major
+//   kPencil   p + (i + i/16) P               pencil-fastest, one pad row per 16
+//   kLinePad  p (N + N/16) + i + i/16        line-major, one pad per 16
+// The thread mapping follows the layout: pencil-fastest tiles put
+// consecutive pencils on consecutive lanes (for data whose pencils are
+// adjacent in memory), line-major ones consecutive indices (for data whose
+// transform axis is contiguous: a half warp then reads 16 consecutive points
+// of one line).  With radix-16 first and last stages both padded layouts are
+// free of bank conflicts.
+constexpr int kLine = 0, kPencil = 1, kLinePad = 2;
 
-    static __device__ __forceinline__ int at(int p, int i) { return PF ? p + (i + (i >> 4)) * P : p * (N + 1) + i; }
+template <int N, int P, int NT, int LY>
+struct FftCT {
+    static constexpr bool PF = LY == kPencil;
+    static constexpr int NST = ct_nst(N);
+    static constexpr int BUF = LY == kLine ? P * (N + 1) : P * (N + N / 16);  // float2 per buffer
+
+    static __device__ __forceinline__ int at(int p, int i)
+    {
+        if constexpr (LY == kPencil) return p + (i + (i >> 4)) * P;
+        else if constexpr (LY == kLinePad) return p * (N + N / 16) + i + (i >> 4);
+        else return p * (N + 1) + i;
+    }
 
     template <int S, bool INV, class Load, class Store>
     static __device__ __forceinline__ void stage(const float2* __restrict__ tw, float2* A, float2* B, Load& load,

@@ -43,12 +43,13 @@ __device__ __forceinline__ long long spec(const KP& k, int kz, int x, int y)
 }
 __device__ __forceinline__ bool in_slab(int i, int n, int pml) { return i < pml || i >= n - pml; }
 
-// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2.
+// Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2.  The
+// address operand is warp-uniform in hardware: issue it from one thread (a
+// per-lane address makes the compiler serialise the lanes).
 __device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes)
 {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
-
 __device__ __forceinline__ void load_table(float2* s, const float2* g, int n)
 {
     for (int i = threadIdx.x; i < n; i += blockDim.x) s[i] = g[i];
@@ -56,19 +57,20 @@ __device__ __forceinline__ void load_table(float2* s, const float2* g, int n)
 
 // A transform of the tile through the compile-time path (N > 0: length N, PC
 // pencils, NT threads) or the runtime one (N == 0: plan pl, prt pencils,
-// layout ps_rt/is_rt).  Pencil-fastest layouts carry one padding row every
-// 16 indices in both paths.
-template <int N, int PC, int NT, bool PF, bool INV, class Load, class Store>
+// layout ps_rt/is_rt).  LY is the shared-memory layout (kLine, kPencil,
+// kLinePad); the padded layouts carry one padding row every 16 indices in
+// both paths.
+template <int N, int PC, int NT, int LY, bool INV, class Load, class Store>
 __device__ __forceinline__ void fft_any(const FftPlan& pl, const float2* tw, float2* A, float2* B, int prt, int ps_rt,
                                         int is_rt, Load load, Store store)
 {
-    if constexpr (N > 0) FftCT<N, PC, NT, PF>::template run<INV>(tw, A, B, load, store);
-    else fft_run<PF>(pl, tw, A, B, prt, ps_rt, is_rt, INV, load, store, PF ? 4 : 0);
+    if constexpr (N > 0) FftCT<N, PC, NT, LY>::template run<INV>(tw, A, B, load, store);
+    else fft_run<LY == kPencil>(pl, tw, A, B, prt, ps_rt, is_rt, INV, load, store, LY == kLine ? 0 : 4);
 }
-template <int N, int PC, int NT, bool PF>
+template <int N, int PC, int NT, int LY>
 __device__ __forceinline__ float2* out_any(const FftPlan& pl, float2* A, float2* B)
 {
-    if constexpr (N > 0) return FftCT<N, PC, NT, PF>::out_buf(A, B);
+    if constexpr (N > 0) return FftCT<N, PC, NT, LY>::out_buf(A, B);
     else return fft_out_buf(pl, A, B);
 }
 
@@ -90,7 +92,7 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int P = N > 0 ? 16 : P_rt;
-    const int n = N > 0 ? N : k.nz, Qp = P / 2, ps = n + 1;
+    const int n = N > 0 ? N : k.nz, Qp = P / 2, ps = n + n / 16;
     float2* tw = sm;
     float2* A = tw + n;
     float2* B = A + Qp * ps;
@@ -98,13 +100,13 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
     __syncthreads();
     const int f = blockIdx.z, x = blockIdx.y, y0 = blockIdx.x * P;
     const float* src = k.v[f];
-    float2* Z = out_any<N, 8, kThreads, false>(k.pz, A, B);
+    float2* Z = out_any<N, 8, kThreads, kLinePad>(k.pz, A, B);
     auto load = [&](int q, int i) -> float2 {
         const long long b = cell(k, x, y0 + 2 * q, i);
         return make_float2(src[b], src[b + n]);
     };
     auto store = [&](int q, int i, float2 v) { Z[q * ps + i] = v; };
-    fft_any<N, 8, kThreads, false, false>(k.pz, tw, A, B, Qp, ps, 1, load, store);
+    fft_any<N, 8, kThreads, kLinePad, false>(k.pz, tw, A, B, Qp, ps, 1, load, store);
     float2* H = k.H[f];
     for (int t = threadIdx.x; t < k.nkz * P; t += blockDim.x) {
         const int p = t % P, kz = t / P, q = p >> 1;
@@ -116,10 +118,11 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
 
 // ------------------------------------------------------------------ k_cy --
 // C2C along y, in place, on L contiguous y lines per block (lines (kz, x)
-// starting at line0).  Pencil-fastest mapping: a warp covers 32/L consecutive
-// points of each of its L lines, so each global access is a full 32-byte
-// sector per line (L = 8) and the shared-memory stages are conflict-free.
-// The field is H[0..2] (forward) or G[0..26] (inverse), by blockIdx.y.
+// starting at line0).  Line-major mapping on a padded tile: each half warp
+// reads or writes 16 consecutive points (128 bytes) of one line, so a warp
+// access touches two lines, and the radix-16 shared-memory stages are
+// conflict-free.  The field is H[0..2] (forward) or G[0..26] (inverse), by
+// blockIdx.y.
 constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
 
 template <int N, bool INV>
@@ -138,7 +141,7 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     float2* base = arr + (line0 + (long long)blockIdx.x * L) * n;
     auto load = [&](int p, int i) -> float2 { return base[(long long)p * n + i]; };
     auto store = [&](int p, int i, float2 v) { base[(long long)p * n + i] = v; };
-    fft_any<N, 8, kCyThreads, true, INV>(k.py, tw, A, B, L, 1, L, load, store);
+    fft_any<N, 8, kCyThreads, kLinePad, INV>(k.py, tw, A, B, L, n + n / 16, 1, load, store);
 }
 
 // ------------------------------------------------------------------ k_mx --
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
         const float2* H = k.H[c];
         auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
         auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
-        fft_any<N, 16, kThreads, true, false>(k.px, tw, A, B, P, 1, P, load, store);
+        fft_any<N, 16, kThreads, kPencil, false>(k.px, tw, A, B, P, 1, P, load, store);
     }
 
     const float kzv = k.kz[kz];
@@ -195,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
                 return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
             };
             auto store = [&](int p, int i, float2 v) { G[spec(k, kz, i, y0 + p)] = v; };
-            fft_any<N, 16, kThreads, true, true>(k.px, tw, A, B, P, 1, P, load, store);
+            fft_any<N, 16, kThreads, kPencil, true>(k.px, tw, A, B, P, 1, P, load, store);
         }
     }
 }
@@ -244,18 +247,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
     const float w0 = k.w0, inv_w0 = 1.0f / k.w0;
     const long long src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
 
-    // L2 prefetch of a group's inputs: the P-row slices of its half spectra
-    // (one 8P-byte run per kz) and the contiguous P*nz runs of the stresses,
-    // loss potentials and coefficients its update reads.  Issued one group
-    // ahead, so each phase's loads hit L2 instead of waiting on HBM.
+    // L2 prefetch of the contiguous P*nz runs of the stresses, loss
+    // potentials and coefficients a group's update reads, issued one group
+    // ahead by one thread.  (The half spectra are read by the transform's
+    // first stage, which keeps 16 loads per thread in flight; prefetching
+    // them 32 bytes at a time cost more instructions than it saved.)
     auto prefetch_group = [&](int g) {
         if (g > 3) return;
-        const int nf = g == 0 ? 9 : 6, of = g == 0 ? 0 : 9 + (g - 1) * 6;
-        const unsigned row = 8u * P;
-        for (int t = threadIdx.x; t < nf * k.nkz; t += blockDim.x) {
-            const int f = t / k.nkz, kz = t - f * k.nkz;
-            prefetch_l2(k.G[of + f] + spec(k, kz, x, y0), row);
-        }
         const long long c0 = cell(k, x, y0, 0);
         const unsigned run = 4u * P * n;
         if (threadIdx.x == 0) {
@@ -295,8 +293,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
             S[(f * P + 2 * q) * np1 + i] = v.x;
             S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        if (grp == 0) fft_any<N, 18, kThreads, true, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
-        else fft_any<N, 12, kThreads, true, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        if (grp == 0) fft_any<N, 18, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        else fft_any<N, 12, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
 
         // 2. stress update of the group.  Each thread owns kCells cells; all
         //    their streaming inputs are loaded before any store so the loads
@@ -485,9 +483,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
             const int f = pp / Qp, q = pp - f * Qp;
             return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
         };
-        float2* Zf = out_any<N, 6, kThreads, false>(k.pz, A, B);
+        float2* Zf = out_any<N, 6, kThreads, kLinePad>(k.pz, A, B);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
-        fft_any<N, 6, kThreads, false, false>(k.pz, tw, A, B, npen, np1, 1, load, store_f);
+        fft_any<N, 6, kThreads, kLinePad, false>(k.pz, tw, A, B, npen, n + n / 16, 1, load, store_f);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
@@ -500,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
             D[(f * P + 2 * q) * np1 + i] = v.x;
             D[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_any<N, 6, kThreads, false, true>(k.pz, tw, X1, Zf, npen, np1, 1, load_i, store_i);
+        fft_any<N, 6, kThreads, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i, store_i);
         for (int t = threadIdx.x; t < 3 * P * n; t += blockDim.x) {
             const int i = t % n, fp = t / n, f = fp / P, p = fp - f * P;
             const int y = y0 + p;
@@ -560,16 +558,16 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 
     // pass 1: sxy + i syy -> dy+ sxy (vx), dy- syy (vy)
     {
-        float2* Zf = out_any<N, 16, kThreads, true>(k.py, A, B);
+        float2* Zf = out_any<N, 16, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int p, int i) -> float2 {
             const long long ip = cell(k, x, i, z0 + p);
             return make_float2(sxy[ip], syy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_any<N, 16, kThreads, true, false>(k.py, tw, A, B, P, 1, P, load, store);
+        fft_any<N, 16, kThreads, kPencil, false>(k.py, tw, A, B, P, 1, P, load, store);
         float2* X1 = Zf == A ? B : A;
         // [2][n][P] in the buffer the last stage does not read
-        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, true>(k.py, X1, Zf));
+        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, kPencil>(k.py, X1, Zf));
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
             return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tF[i], inv_n), cscale(tB[i], inv_n));
@@ -578,7 +576,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
             D[i * P + p] = v.x;
             D[(n + i) * P + p] = v.y;
         };
-        fft_any<N, 16, kThreads, true, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
+        fft_any<N, 16, kThreads, kPencil, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             const long long ip = cell(k, x, i, z);
@@ -603,21 +601,21 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     // pass 2: syz, pencils (2q, 2q+1) -> dy+ syz (vz)
     {
         const int Qp = P / 2;
-        float2* Zf = out_any<N, 8, kThreads, true>(k.py, A, B);
+        float2* Zf = out_any<N, 8, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int q, int i) -> float2 {
             const long long ip = cell(k, x, i, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(syz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_any<N, 8, kThreads, true, false>(k.py, tw, A, B, Qp, 1, Qp, load, store);
+        fft_any<N, 8, kThreads, kPencil, false>(k.py, tw, A, B, Qp, 1, Qp, load, store);
         float2* X1 = Zf == A ? B : A;
-        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, true>(k.py, X1, Zf));  // [n][P]
+        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, kPencil>(k.py, X1, Zf));  // [n][P]
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
             D[i * P + 2 * q] = v.x;
             D[i * P + 2 * q + 1] = v.y;
         };
-        fft_any<N, 8, kThreads, true, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
+        fft_any<N, 8, kThreads, kPencil, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             const long long ip = cell(k, x, i, z);
@@ -677,15 +675,15 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
 
     // pass 1: sxx + i sxy -> dx- sxx (vx), dx+ sxy (vy)
     {
-        float2* Zf = out_any<N, 16, kThreads, true>(k.px, A, B);
+        float2* Zf = out_any<N, 16, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int p, int i) -> float2 {
             const long long ip = cell(k, i, y, z0 + p);
             return make_float2(sxx[ip], sxy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
-        fft_any<N, 16, kThreads, true, false>(k.px, tw, A, B, P, 1, P, load, store);
+        fft_any<N, 16, kThreads, kPencil, false>(k.px, tw, A, B, P, 1, P, load, store);
         float2* X1 = Zf == A ? B : A;
-        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, true>(k.px, X1, Zf));  // [2][n][P]
+        float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, kPencil>(k.px, X1, Zf));  // [2][n][P]
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
             return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tB[i], inv_n), cscale(tF[i], inv_n));
@@ -694,7 +692,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
             D[i * P + p] = v.x;
             D[(n + i) * P + p] = v.y;
         };
-        fft_any<N, 16, kThreads, true, true>(k.px, tw, X1, Zf, P, 1, P, load_i, store_i);
+        fft_any<N, 16, kThreads, kPencil, true>(k.px, tw, X1, Zf, P, 1, P, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
@@ -719,21 +717,21 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     // pass 2: sxz pencils (2q, 2q+1) -> dx+ sxz (vz)
     {
         const int Qp = P / 2;
-        float2* Zf = out_any<N, 8, kThreads, true>(k.px, A, B);
+        float2* Zf = out_any<N, 8, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int q, int i) -> float2 {
             const long long ip = cell(k, i, y, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
-        fft_any<N, 8, kThreads, true, false>(k.px, tw, A, B, Qp, 1, Qp, load, store);
+        fft_any<N, 8, kThreads, kPencil, false>(k.px, tw, A, B, Qp, 1, Qp, load, store);
         float2* X1 = Zf == A ? B : A;
-        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, true>(k.px, X1, Zf));  // [n][P]
+        float* D = reinterpret_cast<float*>(out_any<N, 8, kThreads, kPencil>(k.px, X1, Zf));  // [n][P]
         auto load_i = [&](int q, int i) -> float2 { return cmul(Zf[i * Qp + q], cscale(tF[i], inv_n)); };
         auto store_i = [&](int q, int i, float2 v) {
             D[i * P + 2 * q] = v.x;
             D[i * P + 2 * q + 1] = v.y;
         };
-        fft_any<N, 8, kThreads, true, true>(k.px, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
+        fft_any<N, 8, kThreads, kPencil, true>(k.px, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
@@ -961,7 +959,7 @@ int tile_of(int n, int want)
     return p;
 }
 
-size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + 1)); }
+size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + k.nz / 16)); }
 size_t smem_cy(const KP& k, int L) { return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16)); }
 size_t smem_mx(const KP& k, int P)
 {
