@@ -389,7 +389,10 @@ extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_
     for (int c = 0; c < 3; ++c)
         if (s->d_rec[c]) { s->release(s->d_rec[c]); s->d_rec[c] = nullptr; }
     if (s->alloc(&s->d_rik, nt)) return g_last_error;
-    QV_CUDA(cudaMemcpy(s->d_rik, wavelet, sizeof(float) * nt, cudaMemcpyHostToDevice));
+    // every upload and clear goes through the simulation's stream: it does not
+    // synchronise with the legacy stream, and a pageable upload may return
+    // before its transfer has landed
+    QV_CUDA(cudaMemcpyAsync(s->d_rik, wavelet, sizeof(float) * nt, cudaMemcpyHostToDevice, s->st));
     s->nt = nt;
     KP& k = s->kp;
     k.src_type = type;
@@ -402,7 +405,7 @@ extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_
     if (s->rn > 0)
         for (int c = 0; c < 3; ++c) {
             if (s->alloc(&s->d_rec[c], (size_t)nt * s->rn)) return g_last_error;
-            QV_CUDA(cudaMemset(s->d_rec[c], 0, sizeof(float) * (size_t)nt * s->rn));
+            QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)nt * s->rn, s->st));
             k.rec[c] = s->d_rec[c];
         }
     s->have_src = true;
@@ -428,8 +431,8 @@ extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const 
     k.r_iz = r_iz;
     if (rn > 0) {
         if (s->alloc(&s->d_rix, rn) || s->alloc(&s->d_riy, rn)) return g_last_error;
-        QV_CUDA(cudaMemcpy(s->d_rix, r_ix, sizeof(int) * rn, cudaMemcpyHostToDevice));
-        QV_CUDA(cudaMemcpy(s->d_riy, r_iy, sizeof(int) * rn, cudaMemcpyHostToDevice));
+        QV_CUDA(cudaMemcpyAsync(s->d_rix, r_ix, sizeof(int) * rn, cudaMemcpyHostToDevice, s->st));
+        QV_CUDA(cudaMemcpyAsync(s->d_riy, r_iy, sizeof(int) * rn, cudaMemcpyHostToDevice, s->st));
     }
     k.r_ix = s->d_rix;
     k.r_iy = s->d_riy;
@@ -437,7 +440,7 @@ extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const 
     if (rn > 0 && s->nt > 0)
         for (int c = 0; c < 3; ++c) {
             if (s->alloc(&s->d_rec[c], (size_t)s->nt * rn)) return g_last_error;
-            QV_CUDA(cudaMemset(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * rn));
+            QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * rn, s->st));
             k.rec[c] = s->d_rec[c];
         }
     if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
@@ -599,7 +602,7 @@ extern "C" int qvti_derivative_1d(qvti_sim* s, int axis, int fwd, const float* i
     const size_t b = sizeof(float) * s->ntp;
     QV_CUDA(cudaMalloc(&din, b));
     QV_CUDA(cudaMalloc(&dout, b));
-    QV_CUDA(cudaMemcpy(din, in, b, cudaMemcpyHostToDevice));
+    QV_CUDA(cudaMemcpyAsync(din, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
     launch_derivative_1d(s->kp, axis, fwd, din, dout, s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
@@ -687,7 +690,7 @@ extern "C" int qvti_q_derivative(qvti_sim* s, int axis, int fwd, int power, cons
     const size_t b = sizeof(float) * s->ntp;
     QV_CUDA(cudaMalloc(&din, b));
     QV_CUDA(cudaMalloc(&dout, b));
-    QV_CUDA(cudaMemcpy(din, in, b, cudaMemcpyHostToDevice));
+    QV_CUDA(cudaMemcpyAsync(din, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
     KP k = s->kp;
     k.v[0] = din;
     k.H[0] = s->kp.G[0];  // scratch: rewritten by every time step anyway

@@ -33,14 +33,10 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ long long cell(const KP& k, int x, int y, int z)
-{
-    return ((long long)x * k.ny + y) * k.nz + z;
-}
-__device__ __forceinline__ long long spec(const KP& k, int kz, int x, int y)
-{
-    return ((long long)kz * k.nx + x) * k.ny + y;
-}
+// Element offsets fit in 32 bits: the engine accepts at most 1024^3 cells
+// (qvti_create), and 32-bit offsets take one multiply-add per address.
+__device__ __forceinline__ int cell(const KP& k, int x, int y, int z) { return (x * k.ny + y) * k.nz + z; }
+__device__ __forceinline__ int spec(const KP& k, int kz, int x, int y) { return (kz * k.nx + x) * k.ny + y; }
 __device__ __forceinline__ bool in_slab(int i, int n, int pml) { return i < pml || i >= n - pml; }
 
 // Bulk prefetch of `bytes` (multiple of 16, 16-byte aligned) into L2.  The
@@ -102,7 +98,7 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
     const float* src = k.v[f];
     float2* Z = out_any<N, 8, kThreads, kLinePad>(k.pz, A, B);
     auto load = [&](int q, int i) -> float2 {
-        const long long b = cell(k, x, y0 + 2 * q, i);
+        const int b = cell(k, x, y0 + 2 * q, i);
         return make_float2(src[b], src[b + n]);
     };
     auto store = [&](int q, int i, float2 v) { Z[q * ps + i] = v; };
@@ -225,8 +221,14 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 // stress update; then the z derivatives of the new szz, sxz, syz for the next
 // velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
 // z terms, and the source injection.
+// Resident blocks per SM the register budget is sized for: shared memory
+// already limits a 256-point tile to two blocks and a 512-point one to one,
+// so those get the registers to keep two cells' loads in flight.
+constexpr int sigma_min_blocks(int n) { return n >= 512 ? 1 : n >= 256 ? 2 : 3; }
+constexpr int sigma_cells(int n) { return n == 256 ? 2 : 1; }
+
 template <int N>
-__global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
+__global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
@@ -239,13 +241,31 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
     float2* B = A + bufA;  // aliases S when the transform has two stages
     float* S = reinterpret_cast<float*>(B + (two_buf ? bufA : 0));  // [9][P][np1]
     float* D = S + 9 * P * np1;                                           // [3][P][np1]: szz sxz syz
-    load_table(tw, k.tw_z, n);
-    __syncthreads();
+    float* tz = D + 3 * P * np1;                                          // [4][n]: az bz azh bzh
+    float* ty = tz + 4 * n;                                               // [4][P]: ay by ayh byh of the rows
+    float2* tzs = reinterpret_cast<float2*>(ty + 4 * P);                  // [2][n]: Fz Bz
     const int x = blockIdx.y, y0 = blockIdx.x * P;
+    load_table(tw, k.tw_z, n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        tz[i] = k.az[i];
+        tz[n + i] = k.bz[i];
+        tz[2 * n + i] = k.azh[i];
+        tz[3 * n + i] = k.bzh[i];
+        tzs[i] = k.Fz[i];
+        tzs[n + i] = k.Bz[i];
+    }
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        ty[i] = k.ay[y0 + i];
+        ty[P + i] = k.by[y0 + i];
+        ty[2 * P + i] = k.ayh[y0 + i];
+        ty[3 * P + i] = k.byh[y0 + i];
+    }
+    const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
+    __syncthreads();
     const int it = *k.d_it;
     const float dt = k.dt, inv_dt = 1.0f / k.dt;
     const float w0 = k.w0, inv_w0 = 1.0f / k.w0;
-    const long long src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
+    const int src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
 
     // L2 prefetch of the contiguous P*nz runs of the stresses, loss
     // potentials and coefficients a group's update reads, issued one group
@@ -254,7 +274,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
     // them 32 bytes at a time cost more instructions than it saved.)
     auto prefetch_group = [&](int g) {
         if (g > 3) return;
-        const long long c0 = cell(k, x, y0, 0);
+        const int c0 = cell(k, x, y0, 0);
         const unsigned run = 4u * P * n;
         if (threadIdx.x == 0) {
             if (g == 0) {
@@ -300,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
         //    their streaming inputs are loaded before any store so the loads
         //    are in flight together (the arrays cannot alias, but the
         //    compiler cannot know that through the parameter struct).
-        constexpr int kCells = 1;
+        constexpr int kCells = sigma_cells(N);
         for (int t0 = threadIdx.x; t0 < P * n; t0 += kCells * blockDim.x) {
             if (grp == 0) {
                 float* __restrict__ s0 = k.s[0];
@@ -310,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                 float* __restrict__ q1 = k.Q[1];
                 float* __restrict__ q2 = k.Q[2];
                 float in[kCells][13];
-                long long ipv[kCells];
+                int ipv[kCells];
                 bool ok[kCells];
 #pragma unroll
                 for (int u = 0; u < kCells; ++u) {
@@ -319,7 +339,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                     const int p = t / n, z = t - p * n;
                     ipv[u] = cell(k, x, y0 + p, z);
                     if (ok[u]) {
-                        const long long ip = ipv[u];
+                        const int ip = ipv[u];
                         in[u][0] = s0[ip]; in[u][1] = s1[ip]; in[u][2] = s2[ip];
                         in[u][3] = q0[ip]; in[u][4] = q1[ip]; in[u][5] = q2[ip];
                         in[u][6] = __ldg(k.mrho + ip); in[u][7] = __ldg(k.mgp + ip); in[u][8] = __ldg(k.mgs + ip);
@@ -332,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                     if (!ok[u]) continue;
                     const int t = t0 + u * blockDim.x;
                     const int p = t / n, z = t - p * n, y = y0 + p;
-                    const long long ip = ipv[u];
+                    const int ip = ipv[u];
                     const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
                     auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
                     float sxx = in[u][0], syy = in[u][1], szz = in[u][2];
@@ -381,8 +401,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                         float ph[8];
 #pragma unroll
                         for (int m = 0; m < 8; ++m) {
-                            const float a = m < 3 ? k.ax[x] : (m < 6 ? k.ay[y] : k.az[z]);
-                            const float b = m < 3 ? k.bx[x] : (m < 6 ? k.by[y] : k.bz[z]);
+                            const float a = m < 3 ? axv : (m < 6 ? ty[p] : tz[z]);
+                            const float b = m < 3 ? bxv : (m < 6 ? ty[P + p] : tz[n + z]);
                             const float T = dterm[m] + (qterm[m] - qo[m]) * inv_dt;
                             ph[m] = po[m] + dt * (-a * po[m] - b * T);
                         }
@@ -416,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                 float* __restrict__ sg = k.s[sidx];
                 float* __restrict__ qg = k.Q[sidx];
                 float in[kCells][7];
-                long long ipv[kCells];
+                int ipv[kCells];
                 bool ok[kCells];
 #pragma unroll
                 for (int u = 0; u < kCells; ++u) {
@@ -425,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                     const int p = t / n, z = t - p * n;
                     ipv[u] = cell(k, x, y0 + p, z);
                     if (ok[u]) {
-                        const long long ip = ipv[u];
+                        const int ip = ipv[u];
                         in[u][0] = sg[ip];
                         in[u][1] = qg[ip];
 #pragma unroll
@@ -437,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                     if (!ok[u]) continue;
                     const int t = t0 + u * blockDim.x;
                     const int p = t / n, z = t - p * n, y = y0 + p;
-                    const long long ip = ipv[u];
+                    const int ip = ipv[u];
                     const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
                     auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
                     float sig = in[u][0];
@@ -455,8 +475,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
                         const bool onB = grp == 3 ? in_slab(y, ny, pml) : in_slab(x, nx, pml);
                         const float qoA = onA ? k.qs[mA][ip] : 0.f, poA = onA ? k.phs[mA][ip] : 0.f;
                         const float qoB = onB ? k.qs[mB][ip] : 0.f, poB = onB ? k.phs[mB][ip] : 0.f;
-                        const float aA = grp == 2 ? k.ayh[y] : k.azh[z], bA = grp == 2 ? k.byh[y] : k.bzh[z];
-                        const float aB = grp == 3 ? k.ayh[y] : k.axh[x], bB = grp == 3 ? k.byh[y] : k.bxh[x];
+                        const float aA = grp == 2 ? ty[2 * P + p] : tz[2 * n + z];
+                        const float bA = grp == 2 ? ty[3 * P + p] : tz[3 * n + z];
+                        const float aB = grp == 3 ? ty[2 * P + p] : axhv, bB = grp == 3 ? ty[3 * P + p] : bxhv;
                         const float TA = dA + (qA - qoA) * inv_dt, TB = dB + (qB - qoB) * inv_dt;
                         const float phA = onA ? poA + dt * (-aA * poA - bA * TA) : 0.f;
                         const float phB = onB ? poB + dt * (-aB * poB - bB * TB) : 0.f;
@@ -489,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
-            return cmul(Zf[pp * np1 + i], cscale(f == 0 ? k.Bz[i] : k.Fz[i], inv_n));
+            return cmul(Zf[pp * np1 + i], cscale(f == 0 ? tzs[n + i] : tzs[i], inv_n));
         };
         // derivatives parked in D (its stresses were consumed by stage 0 of
         // the forward transform), then written out with all loads first
@@ -504,14 +525,14 @@ __global__ void __launch_bounds__(kThreads, 3) k_sigma(KP k, int P_rt)
             const int y = y0 + p;
             const int rc = f == 0 ? 2 : f == 1 ? 0 : 1;
             float* __restrict__ ph = k.php[f == 0 ? 8 : f == 1 ? 2 : 5];  // pzz_z, pxz_z, pyz_z
-            const long long ip = cell(k, x, y, i);
+            const int ip = cell(k, x, y, i);
             const bool slab = in_slab(i, n, pml) && i < n - 1 && x < nx - 1 && y < ny - 1;
             const float old = slab ? ph[ip] : 0.f;
             const float part = D[(f * P + p) * np1 + i];
             float r = part;
             if (slab) {
-                const float a = f == 0 ? k.azh[i] : k.az[i];
-                const float b = f == 0 ? k.bzh[i] : k.bz[i];
+                const float a = f == 0 ? tz[2 * n + i] : tz[i];
+                const float b = f == 0 ? tz[3 * n + i] : tz[n + i];
                 const float nw = old + dt * (-a * old - b * part);
                 ph[ip] = nw;
                 r += nw;
@@ -560,7 +581,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int p, int i) -> float2 {
-            const long long ip = cell(k, x, i, z0 + p);
+            const int ip = cell(k, x, i, z0 + p);
             return make_float2(sxy[ip], syy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
@@ -579,7 +600,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         fft_any<N, 16, kThreads, kPencil, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
-            const long long ip = cell(k, x, i, z);
+            const int ip = cell(k, x, i, z);
             const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
             const float r0 = R0[ip], r1 = R1[ip];
             const float p1 = slab ? f1[ip] : 0.f, p4 = slab ? f4[ip] : 0.f;
@@ -603,7 +624,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int q, int i) -> float2 {
-            const long long ip = cell(k, x, i, z0 + 2 * q);
+            const int ip = cell(k, x, i, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(syz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
@@ -618,7 +639,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         fft_any<N, 8, kThreads, kPencil, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
-            const long long ip = cell(k, x, i, z);
+            const int ip = cell(k, x, i, z);
             const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
             const float r2 = R2[ip];
             const float p7 = slab ? f7[ip] : 0.f;
@@ -677,7 +698,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int p, int i) -> float2 {
-            const long long ip = cell(k, i, y, z0 + p);
+            const int ip = cell(k, i, y, z0 + p);
             return make_float2(sxx[ip], sxy[ip]);
         };
         auto store = [&](int p, int i, float2 v) { Zf[i * P + p] = v; };
@@ -696,7 +717,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
-            const long long ip = cell(k, i, y, z);
+            const int ip = cell(k, i, y, z);
             const bool slab = in_slab(i, nx, pml);
             const float a0 = v0[ip], a1 = v1[ip], r0 = R0[ip], r1 = R1[ip], w0 = ri0[ip], w1 = ri1[ip];
             const float p0 = slab ? f0[ip] : 0.f, p3 = slab ? f3[ip] : 0.f;
@@ -719,7 +740,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int q, int i) -> float2 {
-            const long long ip = cell(k, i, y, z0 + 2 * q);
+            const int ip = cell(k, i, y, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
         auto store = [&](int q, int i, float2 v) { Zf[i * Qp + q] = v; };
@@ -735,7 +756,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
             const int p = t % P, i = t / P, z = z0 + p;
             if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
-            const long long ip = cell(k, i, y, z);
+            const int ip = cell(k, i, y, z);
             const bool slab = in_slab(i, nx, pml);
             const float a2 = v2[ip], r2 = R2[ip], w2 = ri2[ip];
             const float p6 = slab ? f6[ip] : 0.f;
@@ -756,7 +777,7 @@ __global__ void k_rec(KP k)
     const int ir = blockIdx.x * blockDim.x + threadIdx.x;
     const int it = *k.d_it;
     if (ir >= k.rn || it < 0 || it >= k.nt_rec) return;
-    const long long ip = cell(k, k.r_ix[ir], k.r_iy[ir], k.r_iz);
+    const int ip = cell(k, k.r_ix[ir], k.r_iy[ir], k.r_iz);
     const long long o = (long long)it * k.rn + ir;
     k.rec[0][o] = k.v[0][ip];
     k.rec[1][o] = k.v[1][ip];
@@ -967,12 +988,13 @@ size_t smem_mx(const KP& k, int P)
 }
 // k_sigma layout: tw[nz] | A | B (only when the z transform has more than two
 // stages; otherwise B aliases S, used only by the final z-derivative pass) |
-// S[9][P][nz+1] | D[3][P][nz+1].
+// S[9][P][nz+1] | D[3][P][nz+1] | z tables [4][nz] | y tables [4][P] | Fz, Bz.
 size_t smem_sigma(const KP& k, int P)
 {
     const size_t bufA = (size_t)9 * (P / 2) * (k.nz + k.nz / 16);
     const int nb = k.pz.nst > 2 ? 2 : 1;
-    return sizeof(float2) * (k.nz + nb * bufA) + sizeof(float) * (size_t)12 * P * (k.nz + 1);
+    return sizeof(float2) * (k.nz + nb * bufA + 2 * k.nz) +
+           sizeof(float) * ((size_t)12 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
 }
 
 size_t smem_vyx(int n, int P) { return sizeof(float2) * (3 * n + 2 * (n + n / 16) * P); }

@@ -62,3 +62,19 @@ def test_q_derivative(qvti, oracle, power, axis, forward):
     ref = _numpy_q_derivative(f, d, axis, forward, power, oracle)
     err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("shape", [(48, 64, 96), (64, 64, 64)])
+def test_q_derivative_repeated_calls(qvti, oracle, shape):
+    """Several calls on one simulation: each call's upload must land before
+    its transforms read it (the uploads are ordered on the simulation's
+    stream)."""
+    d = (10.0, 12.5, 8.0)
+    rng = np.random.default_rng(17)
+    with qvti.Simulation(*shape, 6, *d, 1e-3, 20.0) as sim:
+        for axis, forward, power in [(0, True, -1), (2, False, 1), (1, True, 0), (0, True, -1)]:
+            f = rng.standard_normal(shape).astype(np.float32)
+            out = sim.q_derivative(f, axis, forward, power)
+            ref = _numpy_q_derivative(f, d, axis, forward, power, oracle)
+            err = np.linalg.norm(out - ref) / np.linalg.norm(ref)
+            assert err < 1e-5, (axis, forward, power, err)
