@@ -63,6 +63,11 @@ bool make_plan(int n, FftPlan* p)
         p->nst = 2;
     }
     if (p->nst < 2) return false;
+    // the compile-time transforms (and the shared-memory sizes derived from
+    // them) use the same radix sequence
+    if (p->nst != ct_nst(n)) return false;
+    for (int st = 0; st < p->nst; ++st)
+        if (p->rad[st] != ct_rad(n, st)) return false;
     return true;
 }
 

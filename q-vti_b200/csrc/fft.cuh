@@ -302,13 +302,17 @@ __device__ __forceinline__ float2 unpack_b(float2 z, float2 zmc)
     return make_float2(0.5f * (z.y - zmc.y), -0.5f * (z.x - zmc.x));
 }
 
-// For z = a + i b transformed, the spectrum of M1 a + i M2 b (M1, M2
-// Hermitian multipliers) is 1/2 [(M1+M2) Z(k) + (M1-M2) conj(Z(n-k))].
-__device__ __forceinline__ float2 two_multiplier(float2 z, float2 zmc, float2 m1, float2 m2)
+// For z = a + i b transformed (a, b real), the spectrum of M1 a + i M2 b
+// (M1, M2 Hermitian multipliers) is 1/2 [(M1+M2) Z(k) + (M1-M2) Zc] with
+// Zc = conj(Z(n-k)).  For the staggered-shift pair of one axis, F = i k
+// e^{+i k d/2} and B = i k e^{-i k d/2} satisfy B = (-F.x, F.y) exactly as
+// tabulated (the Nyquist bin of both keeps only its real part), so
+// (M1, M2) = (F, B) (sgn = 1) or (B, F) (sgn = -1) reduces it to
+// i F.y Z + sgn F.x Zc.
+__device__ __forceinline__ float2 two_shift(float2 z, float2 zmc, float2 f, float sgn)
 {
-    float2 sp = cadd(m1, m2), sm = csub(m1, m2);
-    float2 r = cadd(cmul(sp, z), cmul(sm, zmc));
-    return cscale(r, 0.5f);
+    const float fx = sgn * f.x;
+    return make_float2(fmaf(fx, zmc.x, -f.y * z.y), fmaf(fx, zmc.y, f.y * z.x));
 }
 
 }  // namespace qvti

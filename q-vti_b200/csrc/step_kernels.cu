@@ -152,19 +152,30 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int P = N > 0 ? 16 : P_rt;
     const int n = N > 0 ? N : k.nx;
+    // the second transform buffer exists only for transforms of more than
+    // two stages (a two-stage transform reads its input through `load` and
+    // writes its output through `store`)
+    const int nbuf = (N > 0 ? ct_nst(N) : k.px.nst) > 2 ? 2 : 1;
     float2* tw = sm;
     float2* tFx = tw + n;
     float2* tBx = tFx + n;
     float2* V = tBx + n;            // [n][P]
     float2* A = V + n * P;
     float2* B = A + (n + n / 16) * P;
-    float* tkx = reinterpret_cast<float*>(B + (n + n / 16) * P);
+    float2* tFBy = A + nbuf * (n + n / 16) * P;  // [2][P]: Fy, By of the tile's rows
+    float* tkx = reinterpret_cast<float*>(tFBy + 2 * P);
+    float* tky = tkx + n;                         // [P]
+    const int kz = kz0 + blockIdx.y, y0 = blockIdx.x * P, c = blockIdx.z;
     load_table(tw, k.tw_x, n);
     load_table(tFx, k.Fx, n);
     load_table(tBx, k.Bx, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) tkx[i] = k.kx[i];
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        tky[i] = k.ky[y0 + i];
+        tFBy[i] = k.Fy[y0 + i];
+        tFBy[P + i] = k.By[y0 + i];
+    }
     __syncthreads();
-    const int kz = kz0 + blockIdx.y, y0 = blockIdx.x * P, c = blockIdx.z;
 
     {
         const float2* H = k.H[c];
@@ -182,14 +193,14 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
         for (int j = 0; j < 3; ++j) {
             float2* G = k.G[3 * d + j];
             auto load = [&](int p, int i) -> float2 {
-                const float kyv = k.ky[y0 + p];
+                const float kyv = tky[p];
                 const float kxv = tkx[i];
                 float k2 = kxv * kxv + kyv * kyv + kz2;
                 k2 = fmaxf(k2, 1e-10f);  // the reference sets |k|^2 = 1e-10 at DC (cu:74)
                 const float ap = j == 1 ? 1.0f : (j == 0 ? 1.0f / sqrtf(k2) : sqrtf(k2));
                 float2 T;
                 if (ax == 0) T = fw ? tFx[i] : tBx[i];
-                else if (ax == 1) T = fw ? k.Fy[y0 + p] : k.By[y0 + p];
+                else if (ax == 1) T = fw ? tFBy[p] : tFBy[P + p];
                 else T = fw ? tFz : tBz;
                 return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
             };
@@ -555,13 +566,11 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int n = N > 0 ? N : k.ny, ny = n, pml = k.pml;
     float2* tw = sm;
-    float2* tF = tw + n;
-    float2* tB = tF + n;
-    float2* A = tB + n;
+    float2* tF = tw + n;   // forward shift; the backward one is (-F.x, F.y)
+    float2* A = tF + n;
     float2* B = A + (n + n / 16) * P;
     load_table(tw, k.tw_y, n);
     load_table(tF, k.Fy, n);
-    load_table(tB, k.By, n);
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *k.d_it += 1;  // step counter
     __syncthreads();
     const int x = blockIdx.y, z0 = blockIdx.x * P;
@@ -591,7 +600,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, kPencil>(k.py, X1, Zf));
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
-            return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tF[i], inv_n), cscale(tB[i], inv_n));
+            return two_shift(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tF[i], inv_n), 1.0f);
         };
         auto store_i = [&](int p, int i, float2 v) {
             D[i * P + p] = v.x;
@@ -667,13 +676,11 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int n = N > 0 ? N : k.nx, nx = n, pml = k.pml;
     float2* tw = sm;
-    float2* tF = tw + n;
-    float2* tB = tF + n;
-    float2* A = tB + n;
+    float2* tF = tw + n;   // forward shift; the backward one is (-F.x, F.y)
+    float2* A = tF + n;
     float2* B = A + (n + n / 16) * P;
     load_table(tw, k.tw_x, n);
     load_table(tF, k.Fx, n);
-    load_table(tB, k.Bx, n);
     __syncthreads();
     const int y = blockIdx.y, z0 = blockIdx.x * P;
     const float dt = k.dt, inv_n = 1.0f / n;
@@ -707,7 +714,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         float* D = reinterpret_cast<float*>(out_any<N, 16, kThreads, kPencil>(k.px, X1, Zf));  // [2][n][P]
         auto load_i = [&](int p, int i) -> float2 {
             const int im = i ? n - i : 0;
-            return two_multiplier(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tB[i], inv_n), cscale(tF[i], inv_n));
+            return two_shift(Zf[i * P + p], cconj(Zf[im * P + p]), cscale(tF[i], inv_n), -1.0f);
         };
         auto store_i = [&](int p, int i, float2 v) {
             D[i * P + p] = v.x;
@@ -984,7 +991,8 @@ size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2)
 size_t smem_cy(const KP& k, int L) { return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16)); }
 size_t smem_mx(const KP& k, int P)
 {
-    return sizeof(float2) * (3 * k.nx + k.nx * P + 2 * (k.nx + k.nx / 16) * P) + sizeof(float) * k.nx;
+    const int nbuf = k.px.nst > 2 ? 2 : 1;
+    return sizeof(float2) * (3 * k.nx + k.nx * P + nbuf * (k.nx + k.nx / 16) * P + 2 * P) + sizeof(float) * (k.nx + P);
 }
 // k_sigma layout: tw[nz] | A | B (only when the z transform has more than two
 // stages; otherwise B aliases S, used only by the final z-derivative pass) |
@@ -997,7 +1005,7 @@ size_t smem_sigma(const KP& k, int P)
            sizeof(float) * ((size_t)12 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
 }
 
-size_t smem_vyx(int n, int P) { return sizeof(float2) * (3 * n + 2 * (n + n / 16) * P); }
+size_t smem_vyx(int n, int P) { return sizeof(float2) * (2 * n + 2 * (n + n / 16) * P); }
 
 }  // namespace
 
