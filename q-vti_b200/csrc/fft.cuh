@@ -371,6 +371,8 @@ struct FftCT {
     static constexpr int NST = ct_nst(N);
     static constexpr int BUF = LY == kLine ? P * (N + 1) : P * (N + N / 16);  // float2 per buffer
 
+    static constexpr int PSTEP = LY == kPencil ? P : 1;  // distance of consecutive indices
+
     static __device__ __forceinline__ int at(int p, int i)
     {
         if constexpr (LY == kPencil) return p + (i + (i >> 4)) * P;
@@ -396,11 +398,17 @@ struct FftCT {
             else    { j = t % NR; p = t / NR; }
             const int jm = j % NS;
             float2 v[R];
+            if constexpr (FIRST) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int idx = j + r * NR;
-                if constexpr (FIRST) v[r] = load(p, idx);
-                else v[r] = src[at(p, idx)];
+                for (int r = 0; r < R; ++r) v[r] = load(p, j + r * NR);
+            } else if constexpr (LY != kLine && NR % 16 == 0) {
+                // idx = j + r NR: the pad row advances by NR/16 per r
+                const int b = at(p, j);
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[r] = src[b + r * (NR + NR / 16) * PSTEP];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[r] = src[at(p, j + r * NR)];
             }
             if constexpr (!FIRST) {
                 if (jm) {
@@ -413,11 +421,23 @@ struct FftCT {
             }
             Dft<R>::run(v, INV);
             const int base = (j - jm) * R + jm;
+            if constexpr (LAST) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int idx = base + r * NS;
-                if constexpr (LAST) store(p, idx, v[r]);
-                else dst[at(p, idx)] = v[r];
+                for (int r = 0; r < R; ++r) store(p, base + r * NS, v[r]);
+            } else if constexpr (LY != kLine && NS % 16 == 0) {
+                // idx = base + r NS: the pad row advances by NS/16 per r
+                const int b = at(p, base);
+#pragma unroll
+                for (int r = 0; r < R; ++r) dst[b + r * (NS + NS / 16) * PSTEP] = v[r];
+            } else if constexpr (LY != kLine && 16 % (NS * R) == 0) {
+                // the R outputs lie in one aligned run of NS R <= 16 indices
+                // (base = m NS R + jm, jm < NS): one pad row for all of them
+                const int b = at(p, base);
+#pragma unroll
+                for (int r = 0; r < R; ++r) dst[b + r * NS * PSTEP] = v[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) dst[at(p, base + r * NS)] = v[r];
             }
         }
         __syncthreads();

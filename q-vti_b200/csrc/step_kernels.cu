@@ -237,13 +237,14 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 // so those get the registers to keep two cells' loads in flight.
 constexpr int sigma_min_blocks(int n) { return n >= 512 ? 1 : n >= 256 ? 2 : 3; }
 constexpr int sigma_cells(int n) { return n == 256 ? 2 : 1; }
+constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
 
 template <int N>
 __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    const int P = N > 0 ? 4 : P_rt;
+    const int P = N > 0 ? kSigmaRows : P_rt;
     const int n = N > 0 ? N : k.nz, Qp = P / 2, np1 = n + 1, nx = k.nx, ny = k.ny, pml = k.pml;
     const int two_buf = N > 0 ? (ct_nst(N) > 2) : (k.pz.nst > 2);
     const int bufA = 9 * Qp * (n + n / 16);
@@ -324,8 +325,8 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             S[(f * P + 2 * q) * np1 + i] = v.x;
             S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        if (grp == 0) fft_any<N, 18, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
-        else fft_any<N, 12, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        if (grp == 0) fft_any<N, 9 * kSigmaRows / 2, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        else fft_any<N, 6 * kSigmaRows / 2, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
 
         // 2. stress update of the group.  Each thread owns kCells cells; all
         //    their streaming inputs are loaded before any store so the loads
@@ -515,9 +516,9 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             const int f = pp / Qp, q = pp - f * Qp;
             return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
         };
-        float2* Zf = out_any<N, 6, kThreads, kLinePad>(k.pz, A, B);
+        float2* Zf = out_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad>(k.pz, A, B);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
-        fft_any<N, 6, kThreads, kLinePad, false>(k.pz, tw, A, B, npen, n + n / 16, 1, load, store_f);
+        fft_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad, false>(k.pz, tw, A, B, npen, n + n / 16, 1, load, store_f);
         float2* X1 = Zf == A ? B : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
@@ -530,7 +531,8 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             D[(f * P + 2 * q) * np1 + i] = v.x;
             D[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_any<N, 6, kThreads, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i, store_i);
+        fft_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i,
+                                                                 store_i);
         for (int t = threadIdx.x; t < 3 * P * n; t += blockDim.x) {
             const int i = t % n, fp = t / n, f = fp / P, p = fp - f * P;
             const int y = y0 + p;
@@ -1103,7 +1105,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         });
         mark(5);
     }
-    const int Ps = tile_of(k.ny, 4);
+    const int Ps = tile_of(k.ny, kSigmaRows);
     dispatch_len(len(k.nz), [&](auto NN) {
         k_sigma<decltype(NN)::value><<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
     });
