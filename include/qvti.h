@@ -29,7 +29,8 @@ enum {
     QVTI_ERR_UNSUPPORTED = 3, /* grid size / option not supported          */
     QVTI_ERR_STATE = 4,       /* call out of order (e.g. no model set)     */
     QVTI_ERR_OOM = 5,         /* device allocation failed                  */
-    QVTI_ERR_NONFINITE = 6    /* a non-finite value was detected           */
+    QVTI_ERR_NONFINITE = 6,   /* a non-finite value was detected           */
+    QVTI_ERR_TIMEOUT = 7      /* a wait ended before its shot finished     */
 };
 
 enum { QVTI_SRC_FORCE_X = 0, QVTI_SRC_EXPLOSIVE = 1 };
@@ -166,6 +167,84 @@ int qvti_q_derivative_noalloc(const float* d_in, float* d_out, int ntx, int nty,
 int qvti_profile_step(qvti_sim* sim, int nrep, int maxk, int* nkernels, char* names, float* ms, double* bytes);
 
 /* Last error code of this process and its description. */
+/* The simulation's CUDA stream (cudaStream_t), for callers that order their
+ * own work after its steps.  The reference keeps one stream per device
+ * inside struct MultiGPU (cuviscoelas_3D.cu:1168). */
+int qvti_get_stream(qvti_sim* sim, void** stream);
+
+/* kz planes per batch of the k-space passes (1..nz/2+1); a tuning knob for
+ * qvti_autotune.  No counterpart in the reference. */
+int qvti_set_kz_batch(qvti_sim* sim, int kz_batch);
+
+/* ---------------------------------------------------------------------
+ * Batches and serving.  The reference runs shots one after another from a
+ * host loop (viscoelas_3D.cpp:355-405, one cuda_forward_acoustic_3D call per
+ * shot, cuviscoelas_3D.cu:1163-1629); these entry points run many shots of
+ * uneven size on one GPU at once, each on its own stream with its time loop
+ * as CUDA-graph launches, admitted first-in first-out under an HBM budget.
+ * Shots are independent, so each shot's result is the same whether it runs
+ * alone or among others.
+ * --------------------------------------------------------------------- */
+typedef struct {
+    int ntx, nty, ntz, pml;       /* as qvti_config                                   */
+    float dx, dy, dz, dt, f0;
+    int vti;
+    const float *velp, *vels, *rho, *gama_p, *gama_s; /* host, ntx*nty*ntz each      */
+    const float *eps, *delta;     /* host, VTI only (NULL otherwise)                  */
+    int src_type, s_ix, s_iy, s_iz; /* as qvti_set_source                             */
+    const float* wavelet;         /* nt samples                                       */
+    int nt;                       /* steps                                            */
+    int r_iz, rn;                 /* as qvti_set_receivers                            */
+    const int *r_ix, *r_iy;
+    float *rec_vx, *rec_vy, *rec_vz; /* host outputs, nt*rn floats each, [it][ir]; may be NULL */
+} qvti_shot;
+
+typedef struct {
+    int status;        /* QVTI_OK or this shot's error                          */
+    double queue_s;    /* submit -> its steps enqueued on the GPU (host clock)  */
+    double latency_s;  /* submit -> records copied out (host clock)             */
+    float device_ms;   /* first to last step of the shot on the GPU (CUDA events) */
+} qvti_shot_result;
+
+typedef struct {
+    int device;        /* CUDA device ordinal                                   */
+    size_t mem_budget; /* device bytes the scheduler may hold; 0: 90% of free   */
+    int max_active;    /* shots in flight; 0: per grid from qvti_autotune        */
+} qvti_sched_opts;
+
+typedef struct qvti_server qvti_server;
+
+/* Start a serving loop (one scheduler thread) on opts->device. */
+int qvti_server_create(const qvti_sched_opts* opts, qvti_server** out);
+
+/* Queue one shot.  Every array the descriptor points to is borrowed until
+ * qvti_server_wait has returned its ticket.  A shot whose footprint exceeds
+ * the whole budget is rejected with QVTI_ERR_OOM. */
+int qvti_server_submit(qvti_server* srv, const qvti_shot* shot, long long* ticket);
+
+/* Wait for a ticket (timeout_s < 0: no limit).  QVTI_ERR_TIMEOUT if the shot
+ * has not finished in time (the ticket stays valid); otherwise the shot's
+ * result (res->status carries its own error). */
+int qvti_server_wait(qvti_server* srv, long long ticket, double timeout_s, qvti_shot_result* res);
+
+/* Shots waiting plus in flight, and the device bytes the pool holds. */
+int qvti_server_load(qvti_server* srv, int* queued, int* active, size_t* pool_bytes);
+
+/* Finish the shots already submitted, stop the loop, free the pool. */
+int qvti_server_destroy(qvti_server* srv);
+
+/* Run n shots through a serving loop and wait for all; results[n] and the
+ * wall time of the whole batch (host clock). */
+int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_opts* opts, qvti_shot_result* results,
+                   double* wall_s);
+
+/* Probe one grid: run probe_steps steps on 1..max_active concurrent
+ * simulations (homogeneous model) for each kz batch in {nz/2+1, (nz/2+2)/2}
+ * and report the fastest setting and its Gcell-steps/s.  The scheduler
+ * caches the result per grid. */
+int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active, int* best_kz_batch,
+                  double* gcell_steps);
+
 int qvti_last_error(void);
 const char* qvti_error_string(int code);
 

@@ -161,6 +161,7 @@ struct Sim {
     int* d_rix = nullptr;
     int* d_riy = nullptr;
     float* d_rec[3] = {};
+    size_t rik_cap = 0, rix_cap = 0, rec_cap = 0;  // element capacities of the buffers above
     double* d_norm = nullptr;
     int* d_bad = nullptr;
     int nt = 0, rn = 0;
@@ -183,6 +184,18 @@ struct Sim {
     {
         for (auto& q : allocs)
             if (q == p) { cudaFree(q); q = nullptr; }
+    }
+    // Grow-only buffer: reallocated only when `count` exceeds its capacity,
+    // so a simulation reused shot after shot does not call cudaFree (which
+    // can wait for the work of every stream on the device).
+    template <class T>
+    int ensure(T** p, size_t* cap, size_t count)
+    {
+        if (*p && count <= *cap) return QVTI_OK;
+        if (*p) { release(*p); *p = nullptr; *cap = 0; }
+        const int rc = alloc(p, count);
+        if (rc == QVTI_OK) *cap = count;
+        return rc;
     }
     ~Sim()
     {
@@ -363,13 +376,15 @@ extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels,
         for (int i = 0; i < nin; ++i) dev[i] = host[i];
     } else {
         for (int i = 0; i < nin; ++i) {
-            if (s->alloc(&tmp[i], ntp)) return g_last_error;
+            // stream-ordered temporaries: allocating and freeing them does not
+            // synchronise with other simulations' streams
+            QV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp[i]), bytes, s->st));
             QV_CUDA(cudaMemcpyAsync(tmp[i], host[i], bytes, cudaMemcpyHostToDevice, s->st));
             dev[i] = tmp[i];
         }
     }
     float** d_coef = nullptr;
-    QV_CUDA(cudaMalloc(&d_coef, sizeof(float*) * 12));
+    QV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_coef), sizeof(float*) * 12, s->st));
     QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 12, cudaMemcpyHostToDevice, s->st));
     const float w0 = s->kp.w0;
     launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
@@ -377,9 +392,9 @@ extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels,
     launch_mu_rinv(s->kp, dev[2], s->coef + 7, s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
-    cudaFree(d_coef);
+    QV_CUDA(cudaFreeAsync(d_coef, s->st));
     for (int i = 0; i < nin; ++i)
-        if (tmp[i]) s->release(tmp[i]);
+        if (tmp[i]) QV_CUDA(cudaFreeAsync(tmp[i], s->st));
     s->have_model = true;
     return QVTI_OK;
 }
@@ -390,10 +405,7 @@ extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_
     if (!s || !wavelet || nt <= 0 || (type != QVTI_SRC_FORCE_X && type != QVTI_SRC_EXPLOSIVE)) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     QV_CUDA(cudaStreamSynchronize(s->st));
-    if (s->d_rik) { s->release(s->d_rik); s->d_rik = nullptr; }
-    for (int c = 0; c < 3; ++c)
-        if (s->d_rec[c]) { s->release(s->d_rec[c]); s->d_rec[c] = nullptr; }
-    if (s->alloc(&s->d_rik, nt)) return g_last_error;
+    if (s->ensure(&s->d_rik, &s->rik_cap, nt)) return g_last_error;
     // every upload and clear goes through the simulation's stream: it does not
     // synchronise with the legacy stream, and a pageable upload may return
     // before its transfer has landed
@@ -407,12 +419,17 @@ extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_
     k.s_iz = s_iz;
     k.rik = s->d_rik;
     k.nt_rec = nt;
-    if (s->rn > 0)
+    for (int c = 0; c < 3; ++c) k.rec[c] = nullptr;
+    if (s->rn > 0) {
+        size_t cap = s->rec_cap;
         for (int c = 0; c < 3; ++c) {
-            if (s->alloc(&s->d_rec[c], (size_t)nt * s->rn)) return g_last_error;
+            cap = s->rec_cap;
+            if (s->ensure(&s->d_rec[c], &cap, (size_t)nt * s->rn)) return g_last_error;
             QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)nt * s->rn, s->st));
             k.rec[c] = s->d_rec[c];
         }
+        s->rec_cap = cap;
+    }
     s->have_src = true;
     if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     return QVTI_OK;
@@ -426,28 +443,32 @@ extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const 
         if (r_ix[i] < 0 || r_ix[i] >= s->nx || r_iy[i] < 0 || r_iy[i] >= s->ny) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     QV_CUDA(cudaStreamSynchronize(s->st));
-    if (s->d_rix) { s->release(s->d_rix); s->d_rix = nullptr; }
-    if (s->d_riy) { s->release(s->d_riy); s->d_riy = nullptr; }
-    for (int c = 0; c < 3; ++c)
-        if (s->d_rec[c]) { s->release(s->d_rec[c]); s->d_rec[c] = nullptr; }
     KP& k = s->kp;
     s->rn = rn;
     k.rn = rn;
     k.r_iz = r_iz;
     if (rn > 0) {
-        if (s->alloc(&s->d_rix, rn) || s->alloc(&s->d_riy, rn)) return g_last_error;
+        size_t cap = s->rix_cap;
+        if (s->ensure(&s->d_rix, &cap, rn)) return g_last_error;
+        cap = s->rix_cap;
+        if (s->ensure(&s->d_riy, &cap, rn)) return g_last_error;
+        s->rix_cap = cap;
         QV_CUDA(cudaMemcpyAsync(s->d_rix, r_ix, sizeof(int) * rn, cudaMemcpyHostToDevice, s->st));
         QV_CUDA(cudaMemcpyAsync(s->d_riy, r_iy, sizeof(int) * rn, cudaMemcpyHostToDevice, s->st));
     }
     k.r_ix = s->d_rix;
     k.r_iy = s->d_riy;
     for (int c = 0; c < 3; ++c) k.rec[c] = nullptr;
-    if (rn > 0 && s->nt > 0)
+    if (rn > 0 && s->nt > 0) {
+        size_t cap = s->rec_cap;
         for (int c = 0; c < 3; ++c) {
-            if (s->alloc(&s->d_rec[c], (size_t)s->nt * rn)) return g_last_error;
+            cap = s->rec_cap;
+            if (s->ensure(&s->d_rec[c], &cap, (size_t)s->nt * rn)) return g_last_error;
             QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * rn, s->st));
             k.rec[c] = s->d_rec[c];
         }
+        s->rec_cap = cap;
+    }
     if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     return QVTI_OK;
 }
@@ -709,6 +730,24 @@ extern "C" int qvti_q_derivative(qvti_sim* s, int axis, int fwd, int power, cons
     return QVTI_OK;
 }
 
+extern "C" int qvti_get_stream(qvti_sim* s, void** stream)
+{
+    if (!s || !stream) return qvti::fail(QVTI_ERR_ARG);
+    *stream = static_cast<void*>(s->st);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_kz_batch(qvti_sim* s, int kz_batch)
+{
+    using namespace qvti;
+    if (!s || kz_batch < 1 || kz_batch > s->nkz) return fail(QVTI_ERR_ARG);
+    if (s->kp.kz_batch != kz_batch) {
+        s->kp.kz_batch = kz_batch;
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    }
+    return QVTI_OK;
+}
+
 extern "C" int qvti_last_error(void) { return qvti::g_last_error; }
 
 extern "C" const char* qvti_error_string(int code)
@@ -721,6 +760,7 @@ extern "C" const char* qvti_error_string(int code)
         case QVTI_ERR_STATE: return "call out of order";
         case QVTI_ERR_OOM: return "device allocation failed";
         case QVTI_ERR_NONFINITE: return "non-finite value detected";
+        case QVTI_ERR_TIMEOUT: return "wait timed out";
         default: return "unknown error";
     }
 }

@@ -1,0 +1,560 @@
+// Shot scheduler: batches of shots and a continuous serving loop on one GPU.
+//
+// The reference runs its shots one after another from a host loop
+// (viscoelas_3D.cpp:355-405; each shot is one synchronous
+// cuda_forward_acoustic_3D call, cuviscoelas_3D.cu:1163-1629).  Shots are
+// independent, so here many of them -- grids of any supported size -- are in
+// flight on one GPU at once:
+//
+//   * every shot runs on a pooled simulation (one stream each) whose time
+//     loop is a CUDA graph of one step, launched in chunks of kChunk steps
+//     with at most two chunks queued ahead, so a long shot never fills the
+//     launch queue and the scheduler thread stays free;
+//   * shots are admitted first in, first out when a slot and device memory
+//     are free: an idle pooled simulation of the same grid is reused,
+//     otherwise idle simulations are freed (least recently used first) until
+//     the new one fits the budget;
+//   * the number of shots in flight is fixed by the caller, taken from the
+//     per-grid autotuner cache, or bounded by the cells in flight.
+//
+// One scheduler thread issues every engine call of a server; callers only
+// touch the queue and the results under the server's mutex.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "qvti.h"
+
+namespace {
+
+constexpr int kChunk = 16;                      // steps per enqueued chunk
+constexpr long long kCellsInFlight = 1ll << 25;  // default bound: two 256^3 grids
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct GridKey {
+    int ntx, nty, ntz, pml, vti;
+    float dx, dy, dz, dt, f0;
+    auto tie() const { return std::tie(ntx, nty, ntz, pml, vti, dx, dy, dz, dt, f0); }
+    bool operator<(const GridKey& o) const { return tie() < o.tie(); }
+    bool operator==(const GridKey& o) const { return tie() == o.tie(); }
+};
+
+GridKey key_of(const qvti_shot& s) { return {s.ntx, s.nty, s.ntz, s.pml, s.vti, s.dx, s.dy, s.dz, s.dt, s.f0}; }
+
+// Grids that share the transform sizes share the tuning (pml, spacing and dt
+// do not change the launch shapes).
+struct ShapeKey {
+    int ntx, nty, ntz, vti;
+    bool operator<(const ShapeKey& o) const
+    {
+        return std::tie(ntx, nty, ntz, vti) < std::tie(o.ntx, o.nty, o.ntz, o.vti);
+    }
+};
+
+struct Tuning {
+    int active, kz_batch;
+};
+std::mutex g_tune_mu;
+std::map<ShapeKey, Tuning> g_tune;
+
+bool cached_tuning(const ShapeKey& k, Tuning* t)
+{
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    *t = it->second;
+    return true;
+}
+
+qvti_config config_of(const GridKey& k, int device)
+{
+    qvti_config c{};
+    c.ntx = k.ntx; c.nty = k.nty; c.ntz = k.ntz; c.pml = k.pml;
+    c.dx = k.dx; c.dy = k.dy; c.dz = k.dz; c.dt = k.dt; c.f0 = k.f0;
+    c.vti = k.vti; c.device = device; c.w0 = 0.f;
+    return c;
+}
+
+struct PoolSim {
+    qvti_sim* sim = nullptr;
+    GridKey key{};
+    size_t bytes = 0;
+    bool busy = false;
+    double last_used = 0;
+};
+
+struct Job {
+    long long ticket = 0;
+    qvti_shot shot{};
+    double t_submit = 0, t_start = 0;
+    PoolSim* slot = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t chunk[2] = {nullptr, nullptr};
+    int nchunk = 0;  // chunks queued and not known finished (0..2)
+    int enq = 0;     // steps enqueued
+    bool finished = false;  // all steps queued (worker-owned)
+    bool ready = false;     // result available (under the server mutex)
+    qvti_shot_result res{};
+};
+
+size_t shot_bytes(const qvti_shot& s)
+{
+    return qvti_footprint_bytes(s.ntx, s.nty, s.ntz, s.vti) + 3 * sizeof(float) * (size_t)s.nt * (size_t)s.rn;
+}
+
+}  // namespace
+
+struct qvti_server {
+    qvti_sched_opts opts{};
+    size_t budget = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job*> queue;                               // waiting (under mu)
+    std::map<long long, std::unique_ptr<Job>> jobs;       // every uncollected ticket (under mu)
+    int n_active = 0;                                     // under mu
+    size_t pool_bytes = 0;                                // under mu (written by the worker)
+    long long next_ticket = 1;
+    bool stopping = false;
+    // worker-owned
+    std::vector<std::unique_ptr<PoolSim>> pool;
+    std::vector<Job*> active;
+    std::thread worker;
+
+    void loop();
+    bool admit_one();
+    int start(Job* j, PoolSim* ps);
+    void top_up(Job* j);
+    void finish(Job* j, int status);
+    int cap_for(const Job* j, long long active_cells) const;
+    PoolSim* acquire(const Job* j, bool* blocked);
+};
+
+namespace {
+
+void release_events(Job* j)
+{
+    if (j->ev0) cudaEventDestroy(j->ev0);
+    if (j->ev1) cudaEventDestroy(j->ev1);
+    for (auto& e : j->chunk)
+        if (e) cudaEventDestroy(e);
+    j->ev0 = j->ev1 = j->chunk[0] = j->chunk[1] = nullptr;
+}
+
+}  // namespace
+
+// Shots in flight allowed while `j` is at the head of the queue.
+int qvti_server::cap_for(const Job* j, long long active_cells) const
+{
+    if (opts.max_active > 0) return opts.max_active;
+    Tuning t;
+    if (cached_tuning({j->shot.ntx, j->shot.nty, j->shot.ntz, j->shot.vti}, &t)) return t.active;
+    // untuned grid: bound the cells in flight (always admit onto an idle GPU)
+    const long long cells = (long long)j->shot.ntx * j->shot.nty * j->shot.ntz;
+    return (active_cells == 0 || active_cells + cells <= kCellsInFlight) ? n_active + 1 : n_active;
+}
+
+// An idle pooled simulation for the job's grid, or a new one once idle
+// simulations have been freed to make room.  A pooled simulation's bytes are
+// its footprint plus the largest record buffers it has held (they only
+// grow).  *blocked: the memory is held by shots in flight; retry after one
+// finishes.  nullptr without *blocked: creation failed (qvti_last_error).
+PoolSim* qvti_server::acquire(const Job* j, bool* blocked)
+{
+    *blocked = false;
+    const GridKey key = key_of(j->shot);
+    const size_t need = shot_bytes(j->shot);
+    PoolSim* reuse = nullptr;
+    for (auto& p : pool)
+        if (!p->busy && p->key == key && (!reuse || p->bytes > reuse->bytes)) reuse = p.get();
+    const size_t grow = reuse ? (need > reuse->bytes ? need - reuse->bytes : 0) : need;
+    size_t held;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        held = pool_bytes;
+    }
+    while (held + grow > budget) {
+        auto victim = pool.end();
+        for (auto it = pool.begin(); it != pool.end(); ++it)
+            if (!(*it)->busy && it->get() != reuse &&
+                (victim == pool.end() || (*it)->last_used < (*victim)->last_used))
+                victim = it;
+        if (victim == pool.end()) {
+            *blocked = true;
+            std::lock_guard<std::mutex> lk(mu);
+            pool_bytes = held;  // what was freed so far stays freed
+            return nullptr;
+        }
+        qvti_destroy((*victim)->sim);
+        held -= (*victim)->bytes;
+        pool.erase(victim);
+    }
+    if (reuse) {
+        reuse->bytes += grow;
+        std::lock_guard<std::mutex> lk(mu);
+        pool_bytes = held + grow;
+        return reuse;
+    }
+    auto ps = std::make_unique<PoolSim>();
+    const qvti_config cfg = config_of(key, opts.device);
+    if (qvti_create(&cfg, &ps->sim) != QVTI_OK) {
+        std::lock_guard<std::mutex> lk(mu);
+        pool_bytes = held;
+        return nullptr;
+    }
+    ps->key = key;
+    ps->bytes = need;
+    pool.push_back(std::move(ps));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        pool_bytes = held + need;
+    }
+    return pool.back().get();
+}
+
+// Upload the shot's model, source and receivers, then queue its first steps.
+int qvti_server::start(Job* j, PoolSim* ps)
+{
+    const qvti_shot& s = j->shot;
+    qvti_sim* sim = ps->sim;
+    ps->busy = true;
+    j->slot = ps;
+    int rc;
+    Tuning t;
+    if (cached_tuning({s.ntx, s.nty, s.ntz, s.vti}, &t) && (rc = qvti_set_kz_batch(sim, t.kz_batch))) return rc;
+    if ((rc = qvti_set_model(sim, s.velp, s.vels, s.rho, s.gama_p, s.gama_s, s.eps, s.delta, 0))) return rc;
+    if ((rc = qvti_set_receivers(sim, s.r_iz, s.r_ix, s.r_iy, s.rn))) return rc;
+    if ((rc = qvti_set_source(sim, s.src_type, s.s_ix, s.s_iy, s.s_iz, s.wavelet, s.nt))) return rc;
+    if ((rc = qvti_reset(sim))) return rc;
+    void* stv = nullptr;
+    if ((rc = qvti_get_stream(sim, &stv))) return rc;
+    j->st = static_cast<cudaStream_t>(stv);
+    if (cudaEventCreate(&j->ev0) != cudaSuccess || cudaEventCreate(&j->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j->chunk[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&j->chunk[1], cudaEventDisableTiming) != cudaSuccess)
+        return QVTI_ERR_CUDA;
+    if (cudaEventRecord(j->ev0, j->st) != cudaSuccess) return QVTI_ERR_CUDA;
+    j->t_start = now_s();
+    j->res.queue_s = j->t_start - j->t_submit;
+    top_up(j);
+    return QVTI_OK;
+}
+
+// Keep at most two chunks of the job's steps queued on its stream.
+void qvti_server::top_up(Job* j)
+{
+    while (j->enq < j->shot.nt) {
+        if (j->nchunk == 2) {
+            if (cudaEventQuery(j->chunk[0]) == cudaErrorNotReady) return;
+            std::swap(j->chunk[0], j->chunk[1]);
+            j->nchunk = 1;
+        }
+        const int n = std::min(kChunk, j->shot.nt - j->enq);
+        if (qvti_step(j->slot->sim, n) != QVTI_OK) {
+            j->res.status = qvti_last_error();
+            j->enq = j->shot.nt;
+            break;
+        }
+        j->enq += n;
+        cudaEventRecord(j->chunk[j->nchunk++], j->st);
+    }
+    if (j->enq >= j->shot.nt && !j->finished) {
+        cudaEventRecord(j->ev1, j->st);
+        j->finished = true;  // all steps queued; done once ev1 completes
+    }
+}
+
+void qvti_server::finish(Job* j, int status)
+{
+    if (status == QVTI_OK && j->res.status == QVTI_OK) {
+        const cudaError_t e = cudaEventSynchronize(j->ev1);
+        if (e != cudaSuccess) status = QVTI_ERR_CUDA;
+        float ms = 0.f;
+        if (status == QVTI_OK && cudaEventElapsedTime(&ms, j->ev0, j->ev1) == cudaSuccess) j->res.device_ms = ms;
+        if (status == QVTI_OK)
+            status = qvti_get_records(j->slot->sim, j->shot.rec_vx, j->shot.rec_vy, j->shot.rec_vz);
+    }
+    if (j->res.status == QVTI_OK) j->res.status = status;
+    release_events(j);
+    if (j->slot) {
+        j->slot->busy = false;
+        j->slot->last_used = now_s();
+        if (j->res.status != QVTI_OK) {  // do not reuse a simulation left in an unknown state
+            for (auto it = pool.begin(); it != pool.end(); ++it)
+                if (it->get() == j->slot) {
+                    qvti_destroy((*it)->sim);
+                    std::lock_guard<std::mutex> lk(mu);
+                    pool_bytes -= (*it)->bytes;
+                    pool.erase(it);
+                    break;
+                }
+        }
+        j->slot = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    j->res.latency_s = now_s() - j->t_submit;
+    j->ready = true;
+    --n_active;
+    cv_done.notify_all();
+}
+
+// Admit the head of the queue if the slot cap and device memory allow.
+bool qvti_server::admit_one()
+{
+    Job* j;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (queue.empty()) return false;
+        j = queue.front();
+        long long cells = 0;
+        for (Job* a : active) cells += (long long)a->shot.ntx * a->shot.nty * a->shot.ntz;
+        if (n_active >= cap_for(j, cells)) return false;
+    }
+    bool blocked = false;
+    PoolSim* ps = acquire(j, &blocked);
+    if (!ps && blocked) return false;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        queue.pop_front();
+        ++n_active;
+    }
+    active.push_back(j);
+    int rc = QVTI_ERR_OOM;
+    if (ps) rc = start(j, ps);
+    else if (qvti_last_error() != QVTI_OK) rc = qvti_last_error();
+    if (rc != QVTI_OK) {
+        active.pop_back();
+        j->res.status = rc;
+        finish(j, rc);
+    }
+    return true;
+}
+
+void qvti_server::loop()
+{
+    cudaSetDevice(opts.device);
+    for (;;) {
+        // retire finished shots, keep the others fed
+        for (size_t i = 0; i < active.size();) {
+            Job* j = active[i];
+            top_up(j);
+            if (j->finished) {
+                const cudaError_t q = cudaEventQuery(j->ev1);
+                if (q != cudaErrorNotReady) {
+                    active.erase(active.begin() + i);
+                    finish(j, q == cudaSuccess ? QVTI_OK : QVTI_ERR_CUDA);
+                    continue;
+                }
+            }
+            ++i;
+        }
+        while (admit_one()) {
+        }
+        std::unique_lock<std::mutex> lk(mu);
+        if (stopping && queue.empty() && active.empty()) break;
+        if (active.empty() && (queue.empty() || n_active > 0))
+            cv_work.wait_for(lk, std::chrono::milliseconds(50));
+        else
+            cv_work.wait_for(lk, std::chrono::microseconds(100));
+    }
+    for (auto& p : pool) qvti_destroy(p->sim);
+    pool.clear();
+    std::lock_guard<std::mutex> lk(mu);
+    pool_bytes = 0;
+}
+
+extern "C" int qvti_server_create(const qvti_sched_opts* opts, qvti_server** out)
+{
+    if (!opts || !out || opts->max_active < 0) return QVTI_ERR_ARG;
+    *out = nullptr;
+    if (cudaSetDevice(opts->device) != cudaSuccess) return QVTI_ERR_CUDA;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return QVTI_ERR_CUDA;
+    auto* s = new (std::nothrow) qvti_server();
+    if (!s) return QVTI_ERR_OOM;
+    s->opts = *opts;
+    s->budget = opts->mem_budget ? opts->mem_budget : (size_t)(0.9 * (double)free_b);
+    s->worker = std::thread([s] { s->loop(); });
+    *out = s;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_server_submit(qvti_server* srv, const qvti_shot* shot, long long* ticket)
+{
+    if (!srv || !shot || !ticket || shot->nt <= 0 || !shot->wavelet || !shot->velp || !shot->vels || !shot->rho ||
+        !shot->gama_p || !shot->gama_s || (shot->vti && (!shot->eps || !shot->delta)) || shot->rn < 0 ||
+        (shot->rn > 0 && (!shot->r_ix || !shot->r_iy)))
+        return QVTI_ERR_ARG;
+    if (shot_bytes(*shot) > srv->budget) return QVTI_ERR_OOM;
+    auto j = std::make_unique<Job>();
+    j->shot = *shot;
+    j->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stopping) return QVTI_ERR_STATE;
+    j->ticket = srv->next_ticket++;
+    *ticket = j->ticket;
+    srv->queue.push_back(j.get());
+    srv->jobs.emplace(j->ticket, std::move(j));
+    srv->cv_work.notify_one();
+    return QVTI_OK;
+}
+
+extern "C" int qvti_server_wait(qvti_server* srv, long long ticket, double timeout_s, qvti_shot_result* res)
+{
+    if (!srv || !res) return QVTI_ERR_ARG;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->jobs.find(ticket);
+    if (it == srv->jobs.end()) return QVTI_ERR_ARG;
+    Job* j = it->second.get();
+    auto ready = [j] { return j->ready; };
+    if (timeout_s < 0) {
+        srv->cv_done.wait(lk, ready);
+    } else if (!srv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
+        return QVTI_ERR_TIMEOUT;
+    }
+    *res = j->res;
+    srv->jobs.erase(it);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_server_load(qvti_server* srv, int* queued, int* active, size_t* pool_bytes)
+{
+    if (!srv) return QVTI_ERR_ARG;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (queued) *queued = (int)srv->queue.size();
+    if (active) *active = srv->n_active;
+    if (pool_bytes) *pool_bytes = srv->pool_bytes;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_server_destroy(qvti_server* srv)
+{
+    if (!srv) return QVTI_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stopping = true;
+        srv->cv_work.notify_one();
+    }
+    if (srv->worker.joinable()) srv->worker.join();
+    delete srv;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_opts* opts, qvti_shot_result* results,
+                              double* wall_s)
+{
+    if (!shots || n < 0 || !opts || !results) return QVTI_ERR_ARG;
+    if (opts->max_active == 0) {  // tune every grid of the batch once
+        for (int i = 0; i < n; ++i) {
+            const ShapeKey k{shots[i].ntx, shots[i].nty, shots[i].ntz, shots[i].vti};
+            Tuning t;
+            if (cached_tuning(k, &t)) continue;
+            const qvti_config cfg = config_of(key_of(shots[i]), opts->device);
+            int a = 0, b = 0;
+            double g = 0;
+            if (qvti_autotune(&cfg, 4, 8, &a, &b, &g) != QVTI_OK) {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tune[k] = {1, (cfg.ntz / 2 + 1)};
+            }
+        }
+    }
+    qvti_server* srv = nullptr;
+    int rc = qvti_server_create(opts, &srv);
+    if (rc) return rc;
+    const double t0 = now_s();
+    std::vector<long long> tickets(n, -1);
+    for (int i = 0; i < n; ++i) {
+        rc = qvti_server_submit(srv, &shots[i], &tickets[i]);
+        if (rc) {
+            results[i] = qvti_shot_result{};
+            results[i].status = rc;
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (tickets[i] >= 0) qvti_server_wait(srv, tickets[i], -1.0, &results[i]);
+    if (wall_s) *wall_s = now_s() - t0;
+    qvti_server_destroy(srv);
+    for (int i = 0; i < n; ++i)
+        if (results[i].status) return results[i].status;
+    return QVTI_OK;
+}
+
+// ------------------------------------------------------------- autotuner --
+extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active,
+                             int* best_kz_batch, double* gcell_steps)
+{
+    if (!cfg || max_active < 1 || probe_steps < 1 || !best_active || !best_kz_batch || !gcell_steps)
+        return QVTI_ERR_ARG;
+    if (cudaSetDevice(cfg->device) != cudaSuccess) return QVTI_ERR_CUDA;
+    const size_t ntp = (size_t)cfg->ntx * cfg->nty * cfg->ntz;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return QVTI_ERR_CUDA;
+    const size_t per = qvti_footprint_bytes(cfg->ntx, cfg->nty, cfg->ntz, cfg->vti);
+    const int fit = (int)std::min<size_t>((size_t)max_active, std::max<size_t>(1, (size_t)(0.8 * free_b) / per));
+    // homogeneous probe model (Vp 3000, Vs 1700, rho 2200, Qp 100, Qs 50)
+    std::vector<float> vp(ntp, 3000.f), vs(ntp, 1700.f), rho(ntp, 2200.f);
+    std::vector<float> gp(ntp, (float)(std::atan(1.0 / 100.0) / 3.1415926)), gs(ntp, (float)(std::atan(1.0 / 50.0) / 3.1415926));
+    std::vector<float> eps(cfg->vti ? ntp : 0, 0.1f), dl(cfg->vti ? ntp : 0, 0.05f);
+    const int warm = 2, nt = warm + probe_steps;
+    std::vector<float> wav(nt, 0.f);
+    wav[0] = 1.f;
+    std::vector<qvti_sim*> sims;
+    int rc = QVTI_OK;
+    for (int i = 0; i < fit && rc == QVTI_OK; ++i) {
+        qvti_sim* s = nullptr;
+        if ((rc = qvti_create(cfg, &s))) break;
+        sims.push_back(s);
+        rc = qvti_set_model(s, vp.data(), vs.data(), rho.data(), gp.data(), gs.data(), cfg->vti ? eps.data() : nullptr,
+                            cfg->vti ? dl.data() : nullptr, 0);
+        if (!rc) rc = qvti_set_source(s, QVTI_SRC_EXPLOSIVE, cfg->ntx / 2, cfg->nty / 2, cfg->ntz / 2, wav.data(), nt);
+    }
+    if (sims.empty()) return rc ? rc : QVTI_ERR_OOM;
+    const int nkz = cfg->ntz / 2 + 1;
+    const int kzb[2] = {nkz, (nkz + 1) / 2};
+    double best = -1;
+    int ba = 1, bb = nkz;
+    for (int b : kzb) {
+        for (int c = 1; c <= (int)sims.size(); ++c) {
+            for (int i = 0; i < c; ++i) {
+                qvti_set_kz_batch(sims[i], b);
+                qvti_reset(sims[i]);
+                qvti_step(sims[i], warm);
+            }
+            cudaDeviceSynchronize();
+            const double t0 = now_s();
+            for (int i = 0; i < c; ++i) qvti_step(sims[i], probe_steps);
+            if (cudaDeviceSynchronize() != cudaSuccess) { rc = QVTI_ERR_CUDA; break; }
+            const double rate = (double)c * ntp * probe_steps / (now_s() - t0) / 1e9;
+            if (rate > best * 1.02) {  // prefer fewer shots in flight unless clearly faster
+                best = rate;
+                ba = c;
+                bb = b;
+            }
+        }
+        if (b == kzb[1] || kzb[0] == kzb[1]) break;
+    }
+    for (qvti_sim* s : sims) qvti_destroy(s);
+    if (rc) return rc;
+    *best_active = ba;
+    *best_kz_batch = bb;
+    *gcell_steps = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[{cfg->ntx, cfg->nty, cfg->ntz, cfg->vti}] = {ba, bb};
+    return QVTI_OK;
+}

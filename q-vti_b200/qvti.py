@@ -31,6 +31,32 @@ class Config(ctypes.Structure):
                 ("device", ctypes.c_int), ("w0", ctypes.c_float)]
 
 
+class Shot(ctypes.Structure):
+    """qvti_shot: one shot of a batch or a serving request."""
+    _fields_ = [("ntx", ctypes.c_int), ("nty", ctypes.c_int), ("ntz", ctypes.c_int), ("pml", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+                ("dt", ctypes.c_float), ("f0", ctypes.c_float), ("vti", ctypes.c_int),
+                ("velp", ctypes.POINTER(ctypes.c_float)), ("vels", ctypes.POINTER(ctypes.c_float)),
+                ("rho", ctypes.POINTER(ctypes.c_float)), ("gama_p", ctypes.POINTER(ctypes.c_float)),
+                ("gama_s", ctypes.POINTER(ctypes.c_float)), ("eps", ctypes.POINTER(ctypes.c_float)),
+                ("delta", ctypes.POINTER(ctypes.c_float)),
+                ("src_type", ctypes.c_int), ("s_ix", ctypes.c_int), ("s_iy", ctypes.c_int), ("s_iz", ctypes.c_int),
+                ("wavelet", ctypes.POINTER(ctypes.c_float)), ("nt", ctypes.c_int),
+                ("r_iz", ctypes.c_int), ("rn", ctypes.c_int),
+                ("r_ix", ctypes.POINTER(ctypes.c_int)), ("r_iy", ctypes.POINTER(ctypes.c_int)),
+                ("rec_vx", ctypes.POINTER(ctypes.c_float)), ("rec_vy", ctypes.POINTER(ctypes.c_float)),
+                ("rec_vz", ctypes.POINTER(ctypes.c_float))]
+
+
+class ShotResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("queue_s", ctypes.c_double), ("latency_s", ctypes.c_double),
+                ("device_ms", ctypes.c_float)]
+
+
+class SchedOpts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int)]
+
+
 _lib = None
 _F = ctypes.POINTER(ctypes.c_float)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -71,6 +97,17 @@ def lib():
                                                          ctypes.c_float, ctypes.c_float, ctypes.c_float,
                                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, _V]),
             "qvti_profile_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _I, ctypes.c_char_p, _F, _D]),
+            "qvti_get_stream": (ctypes.c_int, [_V, ctypes.POINTER(_V)]),
+            "qvti_set_kz_batch": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_server_create": (ctypes.c_int, [ctypes.POINTER(SchedOpts), ctypes.POINTER(_V)]),
+            "qvti_server_submit": (ctypes.c_int, [_V, ctypes.POINTER(Shot), ctypes.POINTER(ctypes.c_longlong)]),
+            "qvti_server_wait": (ctypes.c_int, [_V, ctypes.c_longlong, ctypes.c_double,
+                                                ctypes.POINTER(ShotResult)]),
+            "qvti_server_load": (ctypes.c_int, [_V, _I, _I, ctypes.POINTER(ctypes.c_size_t)]),
+            "qvti_server_destroy": (ctypes.c_int, [_V]),
+            "qvti_run_batch": (ctypes.c_int, [ctypes.POINTER(Shot), ctypes.c_int, ctypes.POINTER(SchedOpts),
+                                              ctypes.POINTER(ShotResult), _D]),
+            "qvti_autotune": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_int, _I, _I, _D]),
             "qvti_last_error": (ctypes.c_int, []),
             "qvti_error_string": (ctypes.c_char_p, [ctypes.c_int]),
         }
@@ -269,3 +306,114 @@ def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=T
         rec = sim.records()
         state = sim.fields(0, 9) if want_state else None
     return dict(rec=rec, snaps=out, state=state)
+
+
+# ------------------------------------------------------------ batches / serving
+ERR_TIMEOUT = 7
+
+
+class ShotRequest:
+    """A shot for qvti_run_batch / the serving loop: owns the host arrays the
+    C descriptor borrows (model, wavelet, receivers, record outputs).
+
+    ``case`` follows tests/qvti_cases.py (velp, vels, rho, gama_p, gama_s,
+    optional eps/delta, rik, s_ix/s_iy/s_iz, r_iz/r_ix/r_iy, grid and
+    spacing); ``ref_offset`` adds the reference's +10 to s_iz like run_case."""
+
+    def __init__(self, c, nt=None, vti=False, src_type=SRC_FORCE_X, ref_offset=True):
+        self.nt = int(c["nt"] if nt is None else nt)
+        shape = (int(c["ntx"]), int(c["nty"]), int(c["ntz"]))
+        self.keep = [_f32(c[k]).reshape(-1) for k in ("velp", "vels", "rho", "gama_p", "gama_s")]
+        eps = _f32(c["eps"]).reshape(-1) if vti else None
+        delta = _f32(c["delta"]).reshape(-1) if vti else None
+        self.keep += [eps, delta]
+        self.wavelet = _f32(c["rik"])[: self.nt].copy()
+        self.r_ix = np.ascontiguousarray(c["r_ix"], np.int32)
+        self.r_iy = np.ascontiguousarray(c["r_iy"], np.int32)
+        rn = len(self.r_ix)
+        self.rec = np.zeros((3, self.nt, rn), np.float32)
+        d = Shot()
+        d.ntx, d.nty, d.ntz, d.pml = shape + (int(c["pml"]),)
+        d.dx, d.dy, d.dz, d.dt, d.f0 = (float(c[k]) for k in ("dx", "dy", "dz", "dt", "f0"))
+        d.vti = 1 if vti else 0
+        d.velp, d.vels, d.rho, d.gama_p, d.gama_s, d.eps, d.delta = (_fp(a) for a in self.keep)
+        d.src_type = src_type
+        d.s_ix, d.s_iy = int(c["s_ix"]), int(c["s_iy"])
+        d.s_iz = int(c["s_iz"]) + (10 if ref_offset else 0)
+        d.wavelet, d.nt = _fp(self.wavelet), self.nt
+        d.r_iz, d.rn = int(c["r_iz"]), rn
+        d.r_ix = self.r_ix.ctypes.data_as(_I)
+        d.r_iy = self.r_iy.ctypes.data_as(_I)
+        d.rec_vx, d.rec_vy, d.rec_vz = (self.rec[i].ctypes.data_as(_F) for i in range(3))
+        self.desc = d
+        self.cells = shape[0] * shape[1] * shape[2]
+
+
+def _opts(device, mem_budget, max_active):
+    o = SchedOpts()
+    o.device, o.mem_budget, o.max_active = int(device), int(mem_budget), int(max_active)
+    return o
+
+
+def run_batch(requests, max_active=0, mem_budget=0, device=0):
+    """Run ShotRequests through qvti_run_batch; returns (results, wall_s).
+    Records land in each request's ``rec`` ([3, nt, rn])."""
+    n = len(requests)
+    arr = (Shot * n)(*[r.desc for r in requests])
+    res = (ShotResult * n)()
+    wall = ctypes.c_double(0)
+    rc = lib().qvti_run_batch(arr, n, ctypes.byref(_opts(device, mem_budget, max_active)), res, ctypes.byref(wall))
+    _check(rc, "qvti_run_batch")
+    return [dict(status=r.status, queue_s=r.queue_s, latency_s=r.latency_s, device_ms=r.device_ms) for r in res], \
+        wall.value
+
+
+def autotune(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, vti=False, max_active=4, probe_steps=8, device=0):
+    cfg = Config(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, 1 if vti else 0, device, 0.0)
+    a, b, g = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
+    _check(lib().qvti_autotune(ctypes.byref(cfg), max_active, probe_steps, ctypes.byref(a), ctypes.byref(b),
+                               ctypes.byref(g)), "qvti_autotune")
+    return a.value, b.value, g.value
+
+
+class Server:
+    """The continuous serving loop (qvti_server_*): submit shots while others
+    run; wait for them by ticket."""
+
+    def __init__(self, max_active=0, mem_budget=0, device=0):
+        h = _V()
+        _check(lib().qvti_server_create(ctypes.byref(_opts(device, mem_budget, max_active)), ctypes.byref(h)),
+               "qvti_server_create")
+        self.h = h
+        self.pending = {}
+
+    def submit(self, req):
+        t = ctypes.c_longlong(0)
+        _check(lib().qvti_server_submit(self.h, ctypes.byref(req.desc), ctypes.byref(t)), "qvti_server_submit")
+        self.pending[t.value] = req  # keep the borrowed arrays alive
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        r = ShotResult()
+        rc = lib().qvti_server_wait(self.h, ticket, float(timeout), ctypes.byref(r))
+        if rc == ERR_TIMEOUT:
+            return None
+        _check(rc, "qvti_server_wait")
+        self.pending.pop(ticket, None)
+        return dict(status=r.status, queue_s=r.queue_s, latency_s=r.latency_s, device_ms=r.device_ms)
+
+    def load(self):
+        q, a, b = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_size_t(0)
+        _check(lib().qvti_server_load(self.h, ctypes.byref(q), ctypes.byref(a), ctypes.byref(b)), "qvti_server_load")
+        return q.value, a.value, b.value
+
+    def close(self):
+        if self.h:
+            lib().qvti_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

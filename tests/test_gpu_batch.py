@@ -1,0 +1,120 @@
+"""Batches and the serving loop (qvti_run_batch, qvti_server_*): many shots of
+uneven size in flight on one GPU.
+
+Shots are independent and every kernel is deterministic (no atomics, fixed
+reduction order), so each shot's seismograms must be bit-identical whether
+it runs alone (one simulation, run_case) or among others; the tests compare
+with exact equality.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import qvti_cases as qc
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    """Five small shots: different grids (runtime and compile-time transform
+    lengths), isotropic and VTI, force and explosive sources, different nt."""
+    specs = [((32, 32, 32), 6, 70, False, 0), ((48, 32, 40), 6, 90, True, 0), ((32, 48, 32), 6, 60, False, 1),
+             ((64, 64, 64), 8, 80, True, 0), ((40, 40, 40), 6, 100, False, 0)]
+    out = []
+    for i, (n, pml, nt, vti, src) in enumerate(specs):
+        c = qc.heterogeneous_case(n=n, pml=pml, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=nt, f0=30.0, seed=40 + i,
+                                  src=(n[0] // 2, n[1] // 2, n[2] // 2), r_iz=n[2] // 2 - 6, name="b%d" % i)
+        if vti:
+            rng = np.random.default_rng(90 + i)
+            c["eps"] = (0.05 + 0.2 * rng.random(n)).astype(np.float32)
+            c["delta"] = (0.12 * rng.random(n)).astype(np.float32)
+        out.append((c, vti, src))
+    return out
+
+
+@pytest.fixture(scope="module")
+def alone(qvti):
+    return [qvti.run_case(c, vti=vti, src_type=src)["rec"] for c, vti, src in _cases()]
+
+
+def _requests(qvti):
+    return [qvti.ShotRequest(c, vti=vti, src_type=src) for c, vti, src in _cases()]
+
+
+@pytest.mark.parametrize("max_active", [1, 3])
+def test_batch_matches_shots_run_alone(qvti, alone, max_active):
+    reqs = _requests(qvti)
+    results, wall = qvti.run_batch(reqs, max_active=max_active)
+    assert wall > 0
+    for r, req, ref in zip(results, reqs, alone):
+        assert r["status"] == 0
+        assert r["device_ms"] > 0 and r["latency_s"] >= r["queue_s"] >= 0
+        assert np.array_equal(req.rec, ref)
+
+
+def test_batch_with_autotuned_concurrency(qvti, alone):
+    reqs = _requests(qvti)[:2]
+    results, _ = qvti.run_batch(reqs, max_active=0)
+    for r, req, ref in zip(results, reqs, alone[:2]):
+        assert r["status"] == 0
+        assert np.array_equal(req.rec, ref)
+
+
+def test_autotune_reports_a_setting(qvti):
+    active, kzb, rate = qvti.autotune(64, 64, 64, 8, 10.0, 10.0, 10.0, 0.8e-3, 30.0, vti=True, max_active=3,
+                                      probe_steps=4)
+    assert 1 <= active <= 3
+    assert kzb in (33, 17)
+    assert rate > 0
+
+
+def test_server_admits_while_others_run(qvti, alone):
+    """Continuous batching: the later requests arrive while the first runs;
+    results are the same as alone, and a zero-timeout wait on an unfinished
+    shot reports a timeout without consuming the ticket."""
+    reqs = _requests(qvti)
+    with qvti.Server(max_active=2) as srv:
+        t0 = srv.submit(reqs[3])              # 64^3 VTI, the longest
+        assert srv.wait(t0, timeout=0.0) is None
+        tickets = [t0]
+        for r in (reqs[0], reqs[1], reqs[2], reqs[4]):
+            time.sleep(0.01)
+            tickets.append(srv.submit(r))
+        q, a, pool = srv.load()
+        assert a <= 2 and pool > 0
+        res = {t: srv.wait(t, timeout=120.0) for t in tickets}
+    order = [3, 0, 1, 2, 4]
+    for t, i in zip(tickets, order):
+        assert res[t] is not None and res[t]["status"] == 0
+        assert np.array_equal(reqs[i].rec, alone[i])
+
+
+def test_server_budget_admits_one_at_a_time(qvti, alone):
+    """A budget that holds one 64^3 simulation: shots queue for memory, the
+    pool frees idle simulations of other grids, results stay exact."""
+    reqs = _requests(qvti)
+    budget = int(qvti.footprint_bytes(64, 64, 64, True) * 1.2)
+    with qvti.Server(max_active=4, mem_budget=budget) as srv:
+        tickets = [srv.submit(r) for r in reqs]
+        seen_active = 0
+        while True:
+            q, a, pool = srv.load()
+            seen_active = max(seen_active, a)
+            assert pool <= budget
+            if q == 0 and a == 0:
+                break
+            time.sleep(0.002)
+        res = [srv.wait(t, timeout=60.0) for t in tickets]
+    assert seen_active >= 1
+    for r, req, ref in zip(res, reqs, alone):
+        assert r["status"] == 0
+        assert np.array_equal(req.rec, ref)
+
+
+def test_server_rejects_a_shot_beyond_the_budget(qvti):
+    c, vti, src = _cases()[3]
+    req = qvti.ShotRequest(c, vti=vti, src_type=src)
+    with qvti.Server(max_active=1, mem_budget=1 << 20) as srv:
+        with pytest.raises(qvti.QvtiError, match="allocation"):
+            srv.submit(req)
