@@ -9,6 +9,12 @@ cells x steps x ranks / max-over-ranks device time of the K timed steps
 N replicas of the shot with no data-path collective ("scaling": "weak");
 torch.distributed only provides the barrier and the max over ranks.
 
+``--workload batch`` (the batching form: 48 seeded VTI shots over the grids
+128^3, 160x160x128, 192^3, 256x256x192, nt scaled by --nt-scale) and
+``--workload serve`` (the serving form: Poisson arrivals, log-uniform grids
+between 96^3 and 384x384x256, iso/VTI 50/50, 150 GB admission budget) print
+one JSON line each for those forms; the default is the 256^3 step.
+
 ``--impl reference`` times the reference's CPU counterpart: the reference has
 no CPU implementation of the path (it is CUDA + cuFFT), so the arm runs the
 FP64 CPU restatement (oracle/) on all host cores, each step a bounded sample
@@ -361,6 +367,147 @@ def our_arm(args, world, rank, local):
     return 0
 
 
+# ------------------------------------------------------- batching form --
+def _shot_case(md, model, n, pml, dt, nt, src, r_step):
+    rik = md.ricker(nt, dt, F0)
+    gx = np.arange(0, n[0], r_step, dtype=np.int32)
+    gy = np.arange(0, n[1], r_step, dtype=np.int32)
+    c = dict(ntx=n[0], nty=n[1], ntz=n[2], pml=pml, nt=nt, dx=DX, dy=DX, dz=DX, dt=dt, f0=F0, rik=rik,
+             s_ix=int(src[0]), s_iy=int(src[1]), s_iz=int(src[2]), r_iz=pml,
+             r_ix=np.repeat(gx, len(gy)), r_iy=np.tile(gy, len(gx)))
+    c.update(model)
+    return c
+
+
+def batch_arm(args):
+    """48 shots, grids drawn uniformly from {128^3, 160x160x128, 192^3,
+    256x256x192}, each with its own seeded layered VTI model (5 % Gaussian
+    perturbations, 80 m correlation: one field set per grid, rolled by a
+    seeded shift per shot), source uniform in x, y and in the top 20 % below
+    the C-PML, nt ~ U[1000, 2500] x --nt-scale, receivers every 4th surface
+    point.  Runs the batch sequentially (one shot in flight) and with the
+    autotuned scheduler; value = cell-steps of the batch / wall time."""
+    qv = _load("qvti_b200", os.path.join(PKG, "qvti.py"))
+    md = _load("qvti_models", os.path.join(PKG, "models.py"))
+    rng = np.random.default_rng(SEED + 4)
+    shapes = [(128, 128, 128), (160, 160, 128), (192, 192, 192), (256, 256, 192)]
+    pml = 20
+    bases = {n: md.perturbation_bases(n, SEED + 10 + i) for i, n in enumerate(shapes)}
+    reqs, cells = [], 0
+    for i in range(args.shots):
+        n = shapes[int(rng.integers(len(shapes)))]
+        nt = max(1, int(round(int(rng.integers(1000, 2501)) * args.nt_scale)))
+        model = md.perturbed_layered(n, SEED + 100 + i, bases[n], rng.integers(0, n, size=3))
+        dt, _, _ = md.choose_dt(model, DX, F0, DT_NOMINAL, vti=True)
+        top = pml + max(1, int(0.2 * (n[2] - 2 * pml)))
+        src = (rng.integers(pml, n[0] - pml), rng.integers(pml, n[1] - pml), rng.integers(pml, top))
+        reqs.append(qv.ShotRequest(_shot_case(md, model, n, pml, dt, nt, src, 4), vti=True, ref_offset=False))
+        cells += n[0] * n[1] * n[2] * nt
+    del bases
+    seq_res, seq_wall = qv.run_batch(reqs, max_active=1)
+    seq_recs = [r.rec.copy() for r in reqs]
+    res, wall = qv.run_batch(reqs, max_active=0)
+    same = all(np.array_equal(a, r.rec) for a, r in zip(seq_recs, reqs))
+    lat = sorted(r["latency_s"] for r in res)
+    out = {"metric": "Gcell-steps/s, batch of %d uneven VTI shots" % args.shots, "value": cells / wall / 1e9,
+           "unit": UNIT, "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "batching form: grids {128^3, 160x160x128, 192^3, 256x256x192}, layered VTI "
+                                  "with 5%% perturbations, pml %d, nt U[1000,2500] x %g, receivers every 4th "
+                                  "surface point" % (pml, args.nt_scale), "shots": args.shots,
+                      "cell_steps": cells},
+           "wall_s": wall, "sequential": {"value": cells / seq_wall / 1e9, "wall_s": seq_wall},
+           "speedup_vs_sequential": seq_wall / wall, "identical_to_sequential": bool(same),
+           "latency_s": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+           "status_ok": all(r["status"] == 0 for r in res + seq_res)}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# -------------------------------------------------------- serving form --
+def serve_arm(args):
+    """Poisson arrivals (rate --rate per s, for --duration s) of shots with
+    grid axes log-uniform between 96 and 384 (x, y) and 96 and 256 (z),
+    rounded to the nearest even 5-smooth size; nt ~ U[800, 3000] x
+    --nt-scale; isotropic or VTI 50/50; seeded unperturbed layered models;
+    admission by HBM footprint under a 150 GB budget.  A producer thread
+    builds each request's model ahead of its arrival, a collector thread
+    waits for results in submission order; latency is submit to seismograms
+    on the host.  value = aggregate Gcell-steps/s."""
+    import queue
+    import threading
+    qv = _load("qvti_b200", os.path.join(PKG, "qvti.py"))
+    md = _load("qvti_models", os.path.join(PKG, "models.py"))
+    rng = np.random.default_rng(SEED + 5)
+    arrivals, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / args.rate))
+        if t > args.duration:
+            break
+        arrivals.append(t)
+    specs = []
+    for i in range(len(arrivals)):
+        lx, ly, lz = (math.exp(rng.uniform(math.log(96), math.log(hi))) for hi in (384, 384, 256))
+        n = (md.smooth_even(lx), md.smooth_even(ly), md.smooth_even(lz))
+        nt = max(1, int(round(int(rng.integers(800, 3001)) * args.nt_scale)))
+        vti = bool(rng.integers(2))
+        pml = 20
+        src = (int(rng.integers(pml, n[0] - pml)), int(rng.integers(pml, n[1] - pml)), pml + 5)
+        specs.append((n, nt, vti, pml, src, SEED + 1000 + i))
+    ready = queue.Queue(maxsize=6)
+
+    def produce():
+        for n, nt, vti, pml, src, seed in specs:
+            prof = md.layered_profiles(n[2], seed)
+            dt, _, _ = md.choose_dt(prof, DX, F0, DT_NOMINAL, vti=vti)
+            model = md.layered_fast(n, seed, vti=vti)
+            c = _shot_case(md, model, n, pml, dt, nt, src, 8)
+            ready.put((qv.ShotRequest(c, vti=vti, ref_offset=False), n[0] * n[1] * n[2] * nt))
+
+    th = threading.Thread(target=produce, daemon=True)
+    th.start()
+    late = 0.0
+    done = queue.Queue()
+    res = []
+    with qv.Server(max_active=0, mem_budget=int(150e9)) as srv:
+        def collect():  # waits in submission order, releasing each request's host arrays
+            while True:
+                item = done.get()
+                if item is None:
+                    return
+                tk, cs = item
+                res.append((srv.wait(tk, timeout=-1.0), cs))
+
+        col = threading.Thread(target=collect, daemon=True)
+        col.start()
+        t0 = time.perf_counter()
+        for a in arrivals:
+            req, cs = ready.get()
+            now = time.perf_counter() - t0
+            if now < a:
+                time.sleep(a - now)
+            else:
+                late = max(late, now - a)
+            done.put((srv.submit(req), cs))
+            del req
+        done.put(None)
+        col.join()
+        t_end = time.perf_counter() - t0
+    ok = all(r["status"] == 0 for r, _ in res)
+    lat = sorted(r["latency_s"] for r, _ in res)
+    cells = sum(cs for _, cs in res)
+    q = lambda p: lat[min(len(lat) - 1, int(p * len(lat)))]
+    out = {"metric": "shot latency p50/p99 and aggregate Gcell-steps/s, serving", "value": cells / t_end / 1e9,
+           "unit": UNIT, "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
+           "latency_s": {"p50": q(0.5), "p99": q(0.99), "max": lat[-1]},
+           "requests": len(res), "offered_rate_per_s": args.rate, "arrival_window_s": args.duration,
+           "max_submit_lag_s": late, "run_s": t_end, "status_ok": ok,
+           "config": {"workload": "serving form: Poisson %.1f/s, axes log-uniform 96..384 (x,y), 96..256 (z) "
+                                  "rounded to even 5-smooth, nt U[800,3000] x %g, iso/VTI 50/50, layered, pml 20, "
+                                  "150 GB budget" % (args.rate, args.nt_scale)}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,7 +517,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--grid", type=int, default=256, help="cube edge (profiling of smaller cases)")
+    ap.add_argument("--workload", default="step", choices=["step", "batch", "serve"])
+    ap.add_argument("--shots", type=int, default=48, help="batch: number of shots")
+    ap.add_argument("--nt-scale", type=float, default=0.1, help="batch/serve: fraction of the nominal nt")
+    ap.add_argument("--rate", type=float, default=4.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: arrival window (s)")
     args = ap.parse_args()
+    if args.workload == "batch":
+        return batch_arm(args)
+    if args.workload == "serve":
+        return serve_arm(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = dist_setup()

@@ -278,6 +278,9 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.dt = cfg->dt;
     k.inv_ntp = (float)(1.0 / (double)s->ntp);
     k.px = px; k.py = py; k.pz = pz;
+    // every launch of the step must fit the shared memory of one block
+    // (e.g. nz = 512 needs more for its z tiles than an SM offers)
+    if (step_smem_bytes(k) > kMaxSmem) return bail(QVTI_ERR_UNSUPPORTED);
     const long long ntp = s->ntp, nspec = (long long)s->nkz * nx * ny;
 
     // 1D tables

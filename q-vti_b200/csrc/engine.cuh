@@ -86,6 +86,9 @@ struct StepProfile {
     int n = 0;
 };
 void launch_step(const KP& kp, cudaStream_t st, StepProfile* prof = nullptr);
+// Largest dynamic shared memory (bytes) one of the step's launches needs.
+size_t step_smem_bytes(const KP& kp);
+constexpr size_t kMaxSmem = 227 * 1024;
 // coef_out: 7 model arrays (rho gp gs c11 c33 c13 cs) then the 5 S-set arrays
 // (input of the MU average).
 void launch_coef_build(const KP& kp, const float* velp, const float* vels, const float* rho,

@@ -39,7 +39,7 @@
 
 namespace {
 
-constexpr int kChunk = 16;                      // steps per enqueued chunk
+constexpr int kChunk = 32;                      // steps per enqueued chunk
 constexpr long long kCellsInFlight = 1ll << 25;  // default bound: two 256^3 grids
 
 double now_s()

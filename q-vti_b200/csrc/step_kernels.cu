@@ -22,6 +22,7 @@
 // The stress-divergence derivatives need no 3D transform at all: their
 // multiplier depends on one wavenumber component, so IFFT3(M(kx) FFT3(f)) is
 // the 1D spectral derivative along x of every x line (likewise y, z).
+#include <algorithm>
 #include <cstdio>
 #include <type_traits>
 
@@ -232,12 +233,23 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 // stress update; then the z derivatives of the new szz, sxz, syz for the next
 // velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
 // z terms, and the source injection.
-// Resident blocks per SM the register budget is sized for: shared memory
-// already limits a 256-point tile to two blocks and a 512-point one to one,
-// so those get the registers to keep two cells' loads in flight.
-constexpr int sigma_min_blocks(int n) { return n >= 512 ? 1 : n >= 256 ? 2 : 3; }
-constexpr int sigma_cells(int n) { return n == 256 ? 2 : 1; }
+// Resident blocks per SM the register budget is sized for: as many as the
+// tile's shared memory admits (at most 3), so a length whose tiles already
+// limit residency gets the registers to keep more loads in flight.
 constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
+constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
+{
+    const int nb = ct_nst(n) > 2 ? 2 : 1;
+    return 8 * ((size_t)n + (size_t)nb * 9 * (kSigmaRows / 2) * (n + n / 16) + 2 * (size_t)n) +
+           4 * ((size_t)12 * kSigmaRows * (n + 1) + 4 * (size_t)n + 4 * kSigmaRows);
+}
+constexpr int sigma_min_blocks(int n)
+{
+    if (n == 0) return 3;
+    const size_t b = (228 * 1024) / (sigma_smem_ct(n) + 1024);
+    return b < 1 ? 1 : b > 3 ? 3 : (int)b;
+}
+constexpr int sigma_cells(int n) { return n == 256 ? 2 : 1; }
 
 template <int N>
 __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
@@ -1011,9 +1023,10 @@ size_t smem_vyx(int n, int P) { return sizeof(float2) * (2 * n + 2 * (n + n / 16
 
 }  // namespace
 
-// Lengths with a compile-time transform path (grids whose three dimensions
-// are multiples of 16); any other even 2/3/5/7-smooth size takes the runtime
-// path.
+// Transform lengths with a compile-time path (the multiples of 16 among the
+// grids the batching and serving workloads draw, and the common cubes); a
+// kernel takes it when its transform length is listed and its tile fits the
+// grid (see launch_step), otherwise the runtime path.
 template <class F>
 void dispatch_len(int n, F&& f)
 {
@@ -1021,13 +1034,19 @@ void dispatch_len(int n, F&& f)
         case 64: f(std::integral_constant<int, 64>{}); break;
         case 96: f(std::integral_constant<int, 96>{}); break;
         case 128: f(std::integral_constant<int, 128>{}); break;
+        case 144: f(std::integral_constant<int, 144>{}); break;
+        case 160: f(std::integral_constant<int, 160>{}); break;
+        case 192: f(std::integral_constant<int, 192>{}); break;
+        case 240: f(std::integral_constant<int, 240>{}); break;
         case 256: f(std::integral_constant<int, 256>{}); break;
+        case 288: f(std::integral_constant<int, 288>{}); break;
+        case 320: f(std::integral_constant<int, 320>{}); break;
+        case 384: f(std::integral_constant<int, 384>{}); break;
         case 512: f(std::integral_constant<int, 512>{}); break;
         default: f(std::integral_constant<int, 0>{}); break;
     }
 }
-
-bool ct_grid(const KP& k) { return k.nx % 16 == 0 && k.ny % 16 == 0 && k.nz % 16 == 0; }
+constexpr int kCtLengths[] = {0, 64, 96, 128, 144, 160, 192, 240, 256, 288, 320, 384, 512};
 
 int configure_kernels()
 {
@@ -1037,7 +1056,7 @@ int configure_kernels()
         cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         if (r != cudaSuccess) e = r;
     };
-    for (int n : {0, 64, 96, 128, 256, 512})
+    for (int n : kCtLengths)
         dispatch_len(n, [&](auto NN) {
             constexpr int N = decltype(NN)::value;
             set((const void*)k_fz<N>);
@@ -1067,20 +1086,21 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
             prof->kind[prof->n++] = kind;
         }
     };
-    const bool ct = ct_grid(k);
-    auto len = [&](int n) { return ct ? n : 0; };
+    // the compile-time path of a kernel fixes its tile: 16 z rows (k_vy,
+    // k_vx), 16 y rows (k_fz, k_mx), 8 lines (k_cy), kSigmaRows y rows
+    auto len = [&](int n, int tile, int want) { return tile == want ? n : 0; };
     mark(-1);
     const int Pv = tile_of(k.nz, 16);
-    dispatch_len(len(k.ny), [&](auto NN) {
+    dispatch_len(len(k.ny, Pv, 16), [&](auto NN) {
         k_vy<decltype(NN)::value><<<dim3(k.nz / Pv, k.nx), kThreads, smem_vyx(k.ny, Pv), st>>>(k, Pv);
     });
     mark(0);
-    dispatch_len(len(k.nx), [&](auto NN) {
+    dispatch_len(len(k.nx, Pv, 16), [&](auto NN) {
         k_vx<decltype(NN)::value><<<dim3(k.nz / Pv, k.ny), kThreads, smem_vyx(k.nx, Pv), st>>>(k, Pv);
     });
     mark(1);
     const int Pz = tile_of(k.ny, 16);
-    dispatch_len(len(k.nz), [&](auto NN) {
+    dispatch_len(len(k.nz, Pz, 16), [&](auto NN) {
         k_fz<decltype(NN)::value><<<dim3(k.ny / Pz, k.nx, 3), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
     });
     mark(2);
@@ -1091,22 +1111,22 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     for (int kz0 = 0; kz0 < k.nkz; kz0 += batch) {
         const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
         const long long line0 = (long long)kz0 * k.nx;
-        dispatch_len(len(k.ny), [&](auto NN) {
+        dispatch_len(len(k.ny, L, 8), [&](auto NN) {
             k_cy<decltype(NN)::value, false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
         });
         mark(3);
-        dispatch_len(len(k.nx), [&](auto NN) {
+        dispatch_len(len(k.nx, Pm, 16), [&](auto NN) {
             k_mx<decltype(NN)::value><<<dim3(k.ny / Pm, nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
         });
         mark(4);
-        dispatch_len(len(k.ny), [&](auto NN) {
+        dispatch_len(len(k.ny, L, 8), [&](auto NN) {
             k_cy<decltype(NN)::value, true><<<dim3(nb * k.nx / L, kNumG), kCyThreads, smem_cy(k, L), st>>>(k, L,
                                                                                                            line0);
         });
         mark(5);
     }
     const int Ps = tile_of(k.ny, kSigmaRows);
-    dispatch_len(len(k.nz), [&](auto NN) {
+    dispatch_len(len(k.nz, Ps, kSigmaRows), [&](auto NN) {
         k_sigma<decltype(NN)::value><<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
     });
     mark(6);
@@ -1114,6 +1134,20 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         k_rec<<<(k.rn + 255) / 256, 256, 0, st>>>(k);
         mark(7);
     }
+}
+
+// Largest dynamic shared memory of the step's launches for this grid.
+size_t step_smem_bytes(const KP& k)
+{
+    const int Pv = tile_of(k.nz, 16), Pz = tile_of(k.ny, 16), L = tile_of(k.nx, 8), Pm = tile_of(k.ny, 16);
+    const int Ps = tile_of(k.ny, kSigmaRows);
+    size_t m = smem_vyx(k.ny, Pv);
+    m = std::max(m, smem_vyx(k.nx, Pv));
+    m = std::max(m, smem_fz(k, Pz));
+    m = std::max(m, smem_cy(k, L));
+    m = std::max(m, smem_mx(k, Pm));
+    m = std::max(m, smem_sigma(k, Ps));
+    return m;
 }
 
 void launch_coef_build(const KP& k, const float* velp, const float* vels, const float* rho, const float* gp,

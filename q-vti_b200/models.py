@@ -88,6 +88,75 @@ def layered_vti(n=(256, 256, 256), d=10.0, seed=2024, nlayers=6, vp_top=1800.0, 
     return out
 
 
+def layered_profiles(nz, seed, nlayers=6, vp_top=1800.0, vp_bot=4500.0):
+    """1D (depth) profiles of the layered model, with the same per-layer draws
+    as layered_vti: velp, vels, rho, eps, delta, qp, qs, gama_p, gama_s."""
+    rng = np.random.default_rng(seed)
+    vp_l = np.linspace(vp_top, vp_bot, nlayers)
+    eps_l = rng.uniform(0.05, 0.25, nlayers)
+    del_l = rng.uniform(0.0, 0.12, nlayers)
+    qp_l = rng.uniform(30.0, 200.0, nlayers)
+    layer = np.minimum((np.arange(nz) * nlayers) // nz, nlayers - 1)
+    p = dict(velp=vp_l[layer], vels=vp_l[layer] / 1.8, rho=310.0 * vp_l[layer] ** 0.25, eps=eps_l[layer],
+             delta=del_l[layer], qp=qp_l[layer], qs=0.5 * qp_l[layer])
+    p = {k: v.astype(np.float32) for k, v in p.items()}
+    p["gama_p"] = gamma_of_q(p["qp"])
+    p["gama_s"] = gamma_of_q(p["qs"])
+    return p
+
+
+MODEL_FIELDS = ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta")
+
+
+def layered_fast(n, seed, vti=True, nlayers=6):
+    """Unperturbed layered model built by broadcasting its depth profiles
+    (the serving workload's "seeded layered models"): float32 [ix][iy][iz]."""
+    p = layered_profiles(n[2], seed, nlayers)
+    out = {}
+    for k in MODEL_FIELDS[:5] + (MODEL_FIELDS[5:] if vti else ()):
+        a = np.empty(n, np.float32)
+        a[...] = p[k][None, None, :]
+        out[k] = a
+    return out
+
+
+def perturbation_bases(n, seed, corr_m=80.0, d=10.0):
+    """One unit Gaussian random field per model property for grid n, to be
+    shared (shifted) by many shots of that grid (perturbed_layered)."""
+    return {k: gaussian_field(n, corr_m / d, np.random.default_rng([seed, i + 1]))
+            for i, k in enumerate(("velp", "vels", "rho", "eps", "delta", "qp", "qs"))}
+
+
+def perturbed_layered(n, seed, bases, shift, pert=0.05, vti=True):
+    """Layered model with this shot's own layer draws, perturbed by 5 % std
+    with the grid's shared Gaussian fields rolled by `shift` cells."""
+    p = layered_profiles(n[2], seed)
+    out = {}
+    for k in ("velp", "vels", "rho", "eps", "delta", "qp", "qs"):
+        if k in ("eps", "delta") and not vti:
+            continue
+        g = np.roll(bases[k], tuple(int(x) for x in shift), axis=(0, 1, 2))
+        out[k] = np.ascontiguousarray(p[k][None, None, :] * (1.0 + pert * g), np.float32)
+    out["gama_p"] = gamma_of_q(out.pop("qp"))
+    out["gama_s"] = gamma_of_q(out.pop("qs"))
+    return out
+
+
+def smooth_even(x, lo=16):
+    """Nearest even 5-smooth integer (2^a 3^b 5^c) to x, at least lo."""
+    best = None
+    for m in range(max(lo, int(x * 0.8)), int(x * 1.25) + 2):
+        if m % 2:
+            continue
+        r = m
+        for f in (2, 3, 5):
+            while r % f == 0:
+                r //= f
+        if r == 1 and (best is None or abs(m - x) < abs(best - x)):
+            best = m
+    return best
+
+
 def stable_dt(model, d, f0, vti=True):
     """Largest stable dt of the staggered PS leapfrog for this model."""
     dx, dy, dz = (d, d, d) if np.isscalar(d) else d
