@@ -170,11 +170,15 @@ struct Sim {
     cudaGraphExec_t gexec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
+    // Device arrays come from the stream-ordered allocator on the
+    // simulation's own stream: creating or freeing a simulation then orders
+    // only against that stream, where cudaMalloc/cudaFree may wait for the
+    // work of every stream on the device (other shots in flight).
     template <class T>
     int alloc(T** p, size_t count)
     {
         void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+        cudaError_t e = cudaMallocAsync(&q, count * sizeof(T) > 0 ? count * sizeof(T) : 16, st);
         if (e != cudaSuccess) return fail(e == cudaErrorMemoryAllocation ? QVTI_ERR_OOM : QVTI_ERR_CUDA);
         allocs.push_back(q);
         *p = static_cast<T*>(q);
@@ -183,11 +187,10 @@ struct Sim {
     void release(void* p)
     {
         for (auto& q : allocs)
-            if (q == p) { cudaFree(q); q = nullptr; }
+            if (q == p) { cudaFreeAsync(q, st); q = nullptr; }
     }
     // Grow-only buffer: reallocated only when `count` exceeds its capacity,
-    // so a simulation reused shot after shot does not call cudaFree (which
-    // can wait for the work of every stream on the device).
+    // so a simulation reused shot after shot keeps its buffers.
     template <class T>
     int ensure(T** p, size_t* cap, size_t count)
     {
@@ -201,7 +204,8 @@ struct Sim {
     {
         if (gexec) cudaGraphExecDestroy(gexec);
         for (void* p : allocs)
-            if (p) cudaFree(p);
+            if (p) cudaFreeAsync(p, st);
+        if (st) cudaStreamSynchronize(st);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (st) cudaStreamDestroy(st);

@@ -15,7 +15,8 @@
 //     otherwise idle simulations are freed (least recently used first) until
 //     the new one fits the budget;
 //   * the number of shots in flight is fixed by the caller, taken from the
-//     per-grid autotuner cache, or bounded by the cells in flight.
+//     per-grid autotuner cache (plus one slot for a shot being set up), or
+//     bounded by the cells in flight.
 //
 // One scheduler thread issues every engine call of a server; callers only
 // touch the queue and the results under the server's mutex.
@@ -163,8 +164,11 @@ void release_events(Job* j)
 int qvti_server::cap_for(const Job* j, long long active_cells) const
 {
     if (opts.max_active > 0) return opts.max_active;
+    // the autotuner measures steady-state stepping; one more slot lets the
+    // next shot's host set-up (model upload, reset, graph build) overlap the
+    // others' steps instead of leaving the GPU idle between shots
     Tuning t;
-    if (cached_tuning({j->shot.ntx, j->shot.nty, j->shot.ntz, j->shot.vti}, &t)) return t.active;
+    if (cached_tuning({j->shot.ntx, j->shot.nty, j->shot.ntz, j->shot.vti}, &t)) return t.active + 1;
     // untuned grid: bound the cells in flight (always admit onto an idle GPU)
     const long long cells = (long long)j->shot.ntx * j->shot.nty * j->shot.ntz;
     return (active_cells == 0 || active_cells + cells <= kCellsInFlight) ? n_active + 1 : n_active;
