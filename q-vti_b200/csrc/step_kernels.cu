@@ -227,33 +227,43 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
     o[4] = rc2 * g * g * pi * inv_w0;
 }
 
-// z-pencils of one x and P y rows (P/2 pencil pairs): C2R of the 27
-// derivative fields group by group (normal: G 0..8, xz: 9..14, xy: 15..20,
-// yz: 21..26), each group batched into one transform and followed by its
-// stress update; then the z derivatives of the new szz, sxz, syz for the next
-// velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
-// z terms, and the source injection.
+constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
+// A two-stage compile-time length runs its C2R with the in-place last stage
+// (the real field tile S overwrites the staging buffer A) on 288 threads: 9
+// fields x 2 pencils x 16 radix-16 butterflies, one task per thread.  That
+// drops S's own 37 KB (256 points), so three blocks fit an SM instead of two.
+constexpr bool sigma_inplace(int n) { return n > 0 && ct_nst(n) == 2; }
+constexpr int sigma_threads(int n) { return sigma_inplace(n) ? 9 * kSigmaRows / 2 * 16 : kThreads; }
+constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
+{
+    const size_t bufA = (size_t)9 * (kSigmaRows / 2) * (n + n / 16);  // float2
+    const size_t nb = sigma_inplace(n) ? 1 : (ct_nst(n) > 2 ? 2 : 1);
+    const size_t sreal = sigma_inplace(n) ? 0 : (size_t)9 * kSigmaRows * (n + 1);
+    return 8 * ((size_t)n + nb * bufA + 2 * (size_t)n) +
+           4 * (sreal + (size_t)3 * kSigmaRows * (n + 1) + 4 * (size_t)n + 4 * kSigmaRows);
+}
 // Resident blocks per SM the register budget is sized for: as many as the
 // tile's shared memory admits (at most 3), so a length whose tiles already
 // limit residency gets the registers to keep more loads in flight.
-constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
-constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
-{
-    const int nb = ct_nst(n) > 2 ? 2 : 1;
-    return 8 * ((size_t)n + (size_t)nb * 9 * (kSigmaRows / 2) * (n + n / 16) + 2 * (size_t)n) +
-           4 * ((size_t)12 * kSigmaRows * (n + 1) + 4 * (size_t)n + 4 * kSigmaRows);
-}
 constexpr int sigma_min_blocks(int n)
 {
     if (n == 0) return 3;
     const size_t b = (228 * 1024) / (sigma_smem_ct(n) + 1024);
     return b < 1 ? 1 : b > 3 ? 3 : (int)b;
 }
-constexpr int sigma_cells(int n) { return n == 256 ? 2 : 1; }
+constexpr int sigma_cells(int n) { return (n == 256 && !sigma_inplace(n)) ? 2 : 1; }
 
+// z-pencils of one x and P y rows (P/2 pencil pairs): C2R of the 27
+// derivative fields group by group (normal: G 0..8, xz: 9..14, xy: 15..20,
+// yz: 21..26), each group batched into one transform and followed by its
+// stress update; then the z derivatives of the new szz, sxz, syz for the next
+// velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
+// z terms, and the source injection.
 template <int N>
-__global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
+__global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
 {
+    constexpr bool INPLACE = sigma_inplace(N);
+    constexpr int NT = sigma_threads(N);
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
     const int P = N > 0 ? kSigmaRows : P_rt;
@@ -262,9 +272,12 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
     const int bufA = 9 * Qp * (n + n / 16);
     float2* tw = sm;
     float2* A = tw + n;
-    float2* B = A + bufA;  // aliases S when the transform has two stages
-    float* S = reinterpret_cast<float*>(B + (two_buf ? bufA : 0));  // [9][P][np1]
-    float* D = S + 9 * P * np1;                                           // [3][P][np1]: szz sxz syz
+    // S [9][P][np1]: the group's real fields.  In place: S overlays A and
+    // there is no B (the z-derivative pass uses D as its second buffer);
+    // otherwise B aliases S when the transform has two stages.
+    float2* B = A + bufA;
+    float* S = INPLACE ? reinterpret_cast<float*>(A) : reinterpret_cast<float*>(B + (two_buf ? bufA : 0));
+    float* D = INPLACE ? reinterpret_cast<float*>(A + bufA) : S + 9 * P * np1;  // [3][P][np1]: szz sxz syz
     float* tz = D + 3 * P * np1;                                          // [4][n]: az bz azh bzh
     float* ty = tz + 4 * n;                                               // [4][P]: ay by ayh byh of the rows
     float2* tzs = reinterpret_cast<float2*>(ty + 4 * P);                  // [2][n]: Fz Bz
@@ -337,8 +350,13 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             S[(f * P + 2 * q) * np1 + i] = v.x;
             S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        if (grp == 0) fft_any<N, 9 * kSigmaRows / 2, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
-        else fft_any<N, 6 * kSigmaRows / 2, kThreads, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        if constexpr (INPLACE) {
+            if (grp == 0) FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>::template run_inplace<true>(tw, A, load, store);
+            else FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>::template run_inplace<true>(tw, A, load, store);
+        } else {
+            if (grp == 0) fft_any<N, 9 * kSigmaRows / 2, NT, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+            else fft_any<N, 6 * kSigmaRows / 2, NT, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
+        }
 
         // 2. stress update of the group.  Each thread owns kCells cells; all
         //    their streaming inputs are loaded before any store so the loads
@@ -528,10 +546,11 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             const int f = pp / Qp, q = pp - f * Qp;
             return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
         };
-        float2* Zf = out_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad>(k.pz, A, B);
+        float2* B2 = INPLACE ? reinterpret_cast<float2*>(D) : B;  // D is read only by stage 0
+        float2* Zf = out_any<N, 3 * kSigmaRows / 2, NT, kLinePad>(k.pz, A, B2);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
-        fft_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad, false>(k.pz, tw, A, B, npen, n + n / 16, 1, load, store_f);
-        float2* X1 = Zf == A ? B : A;
+        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, false>(k.pz, tw, A, B2, npen, n + n / 16, 1, load, store_f);
+        float2* X1 = Zf == A ? B2 : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
             return cmul(Zf[pp * np1 + i], cscale(f == 0 ? tzs[n + i] : tzs[i], inv_n));
@@ -543,7 +562,7 @@ __global__ void __launch_bounds__(kThreads, sigma_min_blocks(N)) k_sigma(KP k, i
             D[(f * P + 2 * q) * np1 + i] = v.x;
             D[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_any<N, 3 * kSigmaRows / 2, kThreads, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i,
+        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i,
                                                                  store_i);
         for (int t = threadIdx.x; t < 3 * P * n; t += blockDim.x) {
             const int i = t % n, fp = t / n, f = fp / P, p = fp - f * P;
@@ -1011,12 +1030,14 @@ size_t smem_mx(const KP& k, int P)
 // k_sigma layout: tw[nz] | A | B (only when the z transform has more than two
 // stages; otherwise B aliases S, used only by the final z-derivative pass) |
 // S[9][P][nz+1] | D[3][P][nz+1] | z tables [4][nz] | y tables [4][P] | Fz, Bz.
-size_t smem_sigma(const KP& k, int P)
+// In place (two-stage compile-time lengths): tw | A (= S) | D | tables.
+size_t smem_sigma(const KP& k, int P, bool inplace)
 {
     const size_t bufA = (size_t)9 * (P / 2) * (k.nz + k.nz / 16);
-    const int nb = k.pz.nst > 2 ? 2 : 1;
+    const int nb = inplace ? 1 : (k.pz.nst > 2 ? 2 : 1);
+    const size_t sreal = inplace ? 0 : (size_t)9 * P * (k.nz + 1);
     return sizeof(float2) * (k.nz + nb * bufA + 2 * k.nz) +
-           sizeof(float) * ((size_t)12 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
+           sizeof(float) * (sreal + (size_t)3 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
 }
 
 size_t smem_vyx(int n, int P) { return sizeof(float2) * (2 * n + 2 * (n + n / 16) * P); }
@@ -1127,7 +1148,8 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     }
     const int Ps = tile_of(k.ny, kSigmaRows);
     dispatch_len(len(k.nz, Ps, kSigmaRows), [&](auto NN) {
-        k_sigma<decltype(NN)::value><<<dim3(k.ny / Ps, k.nx), kThreads, smem_sigma(k, Ps), st>>>(k, Ps);
+        constexpr int N = decltype(NN)::value;
+        k_sigma<N><<<dim3(k.ny / Ps, k.nx), sigma_threads(N), smem_sigma(k, Ps, sigma_inplace(N)), st>>>(k, Ps);
     });
     mark(6);
     if (k.rn > 0) {
@@ -1146,7 +1168,7 @@ size_t step_smem_bytes(const KP& k)
     m = std::max(m, smem_fz(k, Pz));
     m = std::max(m, smem_cy(k, L));
     m = std::max(m, smem_mx(k, Pm));
-    m = std::max(m, smem_sigma(k, Ps));
+    m = std::max(m, smem_sigma(k, Ps, false));  // the larger layout
     return m;
 }
 
