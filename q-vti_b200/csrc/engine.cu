@@ -216,7 +216,7 @@ namespace {
 
 // Number of full-grid float arrays and half-spectrum complex arrays.
 constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 12 + 5 + 3;
-constexpr int kSpecArrays = 3 + kNumG;
+constexpr int kSpecArrays = 3 + 3 + kNumGxy;  // H, Hy, G without the kz-only fields
 
 int build_graph(Sim* s)
 {
@@ -325,7 +325,11 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     for (int c = 0; c < 3; ++c) rc |= s->alloc(&rinv[c], ntp);
     for (int c = 0; c < 12; ++c) rc |= s->alloc(&s->coef[c], ntp);
     for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.H[c], nspec);
-    for (int c = 0; c < kNumG; ++c) rc |= s->alloc(&k.G[c], nspec);
+    for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.Hy[c], nspec);
+    for (int c = 0; c < kNumG; ++c) {
+        k.G[c] = nullptr;
+        if (!is_gz(c)) rc |= s->alloc(&k.G[c], nspec);
+    }
     rc |= s->alloc(&s->d_it, 1);
     rc |= s->alloc(&s->d_norm, 16);
     rc |= s->alloc(&s->d_bad, 4);
@@ -660,9 +664,9 @@ static void kernel_bytes(const qvti_sim* s, double* b)
     b[1] = 3 * F + 6 * F + 3 * F + 3 * F + 24 * cx;                        // k_vx
     b[2] = 3 * F + 3 * S;                                                  // k_fz
     b[3] = 3 * 2 * S;                                                      // k_cy_fwd
-    b[4] = 3 * S + qvti::kNumG * S;                                        // k_mx
-    b[5] = qvti::kNumG * 2 * S;                                            // k_cy_inv
-    // k_sigma: 27 half spectra, 6 stresses and 6 loss potentials read+written,
+    b[4] = 3 * S + qvti::kNumGxy * S;                                      // k_mx
+    b[5] = qvti::kNumGxy * 2 * S;                                          // k_cy_inv
+    // k_sigma: 27 half spectra (24 G, 3 H), 6 stresses and 6 loss potentials read+written,
     // model + MU, 3 R written, C-PML variables in their slabs
     b[6] = qvti::kNumG * S + 12 * F + 12 * F + model + 5 * F + 3 * F + 3 * 8 * cz +
            (48 + 16 + 16) * cx + (48 + 16 + 16) * cy + (32 + 16 + 16) * cz;

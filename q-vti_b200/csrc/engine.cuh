@@ -20,8 +20,11 @@
 //              8-point averaged shear set), 1/rho-bar per velocity component;
 //              built once per shot in FP64 and rounded              float
 //   H[3]       velocity spectra, half along z: [kz][x][y], nkz = nz/2+1 float2
+//   Hy[3]      the same, transformed along y too: [kz][x][ky]       float2
 //   G[27]      9 directional derivatives x 3 dispersion operators
-//              (|k|^-1, 1, |k|) of the velocity spectra, [kz][x][y] float2
+//              (|k|^-1, 1, |k|) of the velocity spectra, [kz][x][y]; the
+//              three whose multiplier depends on kz alone (kGz) are not
+//              stored: k_sigma forms them from H                      float2
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -31,6 +34,13 @@
 namespace qvti {
 
 constexpr int kNumG = 27;
+// G indices o = 3 d + j of the z derivatives with the identity dispersion
+// operator (d = 2 dz vz, 3 dz vx, 7 dz vy; j = 1): their multiplier
+// i kz e^{+-i kz dz/2} depends on kz alone, so IFFT3(M FFT3(v)) is a z
+// transform of H -- they skip the x and y passes.
+constexpr int kGz[3] = {7, 10, 22};
+constexpr int kNumGxy = kNumG - 3;  // fields that go through k_mx and k_cy
+__host__ __device__ constexpr bool is_gz(int o) { return o == 7 || o == 10 || o == 22; }
 
 struct KP {
     int nx, ny, nz, nkz, pml;
@@ -65,6 +75,7 @@ struct KP {
     const float* rinv[3];
     // spectra
     float2* H[3];
+    float2* Hy[3];
     float2* G[kNumG];
     // source and receivers
     int src_type, s_ix, s_iy, s_iz;

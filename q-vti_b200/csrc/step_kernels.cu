@@ -79,6 +79,8 @@ __device__ __forceinline__ float2* out_any(const FftPlan& pl, float2* A, float2*
 __constant__ int c_comp[9] = {0, 1, 2, 0, 2, 0, 1, 1, 2};
 __constant__ int c_axis[9] = {0, 1, 2, 2, 0, 1, 0, 2, 1};
 __constant__ int c_fwd[9] = {1, 1, 1, 0, 0, 0, 0, 0, 0};
+// G indices that go through the x and y passes (all but kGz)
+__constant__ int c_gxy[kNumGxy] = {0, 1, 2, 3, 4, 5, 6, 8, 9, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 23, 24, 25, 26};
 
 // ------------------------------------------------------------------ k_fz --
 // R2C along z of vx, vy, vz.  Tile: one x, P consecutive y rows (P even);
@@ -134,10 +136,13 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     float2* B = A + L * (n + n / 16);
     load_table(tw, k.tw_y, n);
     __syncthreads();
-    float2* arr = INV ? k.G[blockIdx.y] : k.H[blockIdx.y];
-    float2* base = arr + (line0 + (long long)blockIdx.x * L) * n;
-    auto load = [&](int p, int i) -> float2 { return base[(long long)p * n + i]; };
-    auto store = [&](int p, int i, float2 v) { base[(long long)p * n + i] = v; };
+    // forward: H -> Hy (H stays for k_sigma's kz-only fields); inverse: G in
+    // place, blockIdx.y over the fields that went through k_mx
+    const long long off = (line0 + (long long)blockIdx.x * L) * n;
+    const float2* src = (INV ? k.G[c_gxy[blockIdx.y]] : k.H[blockIdx.y]) + off;
+    float2* dst = (INV ? k.G[c_gxy[blockIdx.y]] : k.Hy[blockIdx.y]) + off;
+    auto load = [&](int p, int i) -> float2 { return src[(long long)p * n + i]; };
+    auto store = [&](int p, int i, float2 v) { dst[(long long)p * n + i] = v; };
     fft_any<N, 8, kCyThreads, kLinePad, INV>(k.py, tw, A, B, L, n + n / 16, 1, load, store);
 }
 
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
     __syncthreads();
 
     {
-        const float2* H = k.H[c];
+        const float2* H = k.Hy[c];
         auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
         auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
         fft_any<N, 16, kThreads, kPencil, false>(k.px, tw, A, B, P, 1, P, load, store);
@@ -192,6 +197,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
         if (c_comp[d] != c) continue;
         const int ax = c_axis[d], fw = c_fwd[d];
         for (int j = 0; j < 3; ++j) {
+            if (is_gz(3 * d + j)) continue;  // formed from H in k_sigma
             float2* G = k.G[3 * d + j];
             auto load = [&](int p, int i) -> float2 {
                 const float kyv = tky[p];
@@ -300,6 +306,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
     __syncthreads();
     const int it = *k.d_it;
+    const float inv_nz = 1.0f / n;
     const float dt = k.dt, inv_dt = 1.0f / k.dt;
     const float w0 = k.w0, inv_w0 = 1.0f / k.w0;
     const int src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
@@ -336,11 +343,20 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
+        // a kz-only field (is_gz) is M(kz) H(kz) / nz: the same value the x
+        // and y round trip (normalised by 1/ntp) would have produced
         auto load = [&](int pp, int i) -> float2 {
-            const int f = pp / Qp, q = pp - f * Qp;
+            const int f = pp / Qp, q = pp - f * Qp, o = o0 + f;
             const int kk = i <= n / 2 ? i : n - i;
-            const float4 gg = *reinterpret_cast<const float4*>(k.G[o0 + f] + spec(k, kk, x, y0 + 2 * q));
+            const bool gz = is_gz(o);
+            const float2* src = gz ? k.H[o == 7 ? 2 : o == 10 ? 0 : 1] : k.G[o];
+            const float4 gg = *reinterpret_cast<const float4*>(src + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
+            if (gz) {  // o == 7: forward shift (dz vz); 10, 22: backward
+                const float2 m = cscale(tzs[(o == 7 ? 0 : n) + kk], inv_nz);
+                a = cmul(a, m);
+                b = cmul(b, m);
+            }
             if (kk == 0 || 2 * kk == n) { a.y = 0.f; b.y = 0.f; }
             if (i > n / 2) { a.y = -a.y; b.y = -b.y; }
             return make_float2(a.x - b.y, a.y + b.x);
@@ -1141,7 +1157,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         });
         mark(4);
         dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, true><<<dim3(nb * k.nx / L, kNumG), kCyThreads, smem_cy(k, L), st>>>(k, L,
+            k_cy<decltype(NN)::value, true><<<dim3(nb * k.nx / L, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L,
                                                                                                            line0);
         });
         mark(5);
@@ -1189,8 +1205,10 @@ void launch_mu_rinv(const KP& k, const float* rho, const float* const* sset, cud
 }
 
 // k.v[0] = input field, k.H[0] = k.G[0] = half-spectrum scratch (nkz*nx*ny).
-void launch_q_derivative(const KP& k, int axis, int fwd, int pw, float* out, cudaStream_t st)
+void launch_q_derivative(const KP& k_in, int axis, int fwd, int pw, float* out, cudaStream_t st)
 {
+    KP k = k_in;
+    k.Hy[0] = k.H[0];  // the forward y pass works in place on the one scratch spectrum
     const int Pz = tile_of(k.ny, 16);
     k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
     const int L = tile_of(k.nx, 8);
