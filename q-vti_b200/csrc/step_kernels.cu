@@ -33,6 +33,7 @@ namespace qvti {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kEpi = 4;  // cells per thread and trip in the velocity-kernel epilogues
 
 // Element offsets fit in 32 bits: the engine accepts at most 1024^3 cells
 // (qvti_create), and 32-bit offsets take one multiply-add per address.
@@ -656,24 +657,42 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
             D[(n + i) * P + p] = v.y;
         };
         fft_any<N, 16, kThreads, kPencil, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
-        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
-            const int p = t % P, i = t / P, z = z0 + p;
-            const int ip = cell(k, x, i, z);
-            const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
-            const float r0 = R0[ip], r1 = R1[ip];
-            const float p1 = slab ? f1[ip] : 0.f, p4 = slab ? f4[ip] : 0.f;
-            const float dx = D[i * P + p], dy = D[(n + i) * P + p];
-            float rx = r0 + dx, ry = r1 + dy;
-            if (slab) {
-                const float q1 = p1 + dt * (-k.ay[i] * p1 - k.by[i] * dx);
-                const float q4 = p4 + dt * (-k.ayh[i] * p4 - k.byh[i] * dy);
-                rx += q1;
-                ry += q4;
-                f1[ip] = q1;
-                f4[ip] = q4;
+        // kEpi cells per thread and trip: all their loads are in flight at once
+        for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
+            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            bool ok[kEpi], slab[kEpi];
+            float r0[kEpi], r1[kEpi], p1[kEpi], p4[kEpi];
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                const int t = t0 + u * blockDim.x;
+                ok[u] = t < n * P;
+                pu[u] = t % P;
+                iu[u] = t / P;
+                const int z = z0 + pu[u];
+                ipu[u] = cell(k, x, iu[u], z);
+                slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
+                r0[u] = ok[u] ? R0[ipu[u]] : 0.f;
+                r1[u] = ok[u] ? R1[ipu[u]] : 0.f;
+                p1[u] = slab[u] ? f1[ipu[u]] : 0.f;
+                p4[u] = slab[u] ? f4[ipu[u]] : 0.f;
             }
-            R0[ip] = rx;
-            R1[ip] = ry;
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                if (!ok[u]) continue;
+                const int i = iu[u], p = pu[u], ip = ipu[u];
+                const float dx = D[i * P + p], dy = D[(n + i) * P + p];
+                float rx = r0[u] + dx, ry = r1[u] + dy;
+                if (slab[u]) {
+                    const float q1 = p1[u] + dt * (-k.ay[i] * p1[u] - k.by[i] * dx);
+                    const float q4 = p4[u] + dt * (-k.ayh[i] * p4[u] - k.byh[i] * dy);
+                    rx += q1;
+                    ry += q4;
+                    f1[ip] = q1;
+                    f4[ip] = q4;
+                }
+                R0[ip] = rx;
+                R1[ip] = ry;
+            }
         }
         __syncthreads();
     }
@@ -695,20 +714,35 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
             D[i * P + 2 * q + 1] = v.y;
         };
         fft_any<N, 8, kThreads, kPencil, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
-        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
-            const int p = t % P, i = t / P, z = z0 + p;
-            const int ip = cell(k, x, i, z);
-            const bool slab = in_slab(i, ny, pml) && xin && i < ny - 1 && z < k.nz - 1;
-            const float r2 = R2[ip];
-            const float p7 = slab ? f7[ip] : 0.f;
-            const float dz = D[i * P + p];
-            float rz = r2 + dz;
-            if (slab) {
-                const float q7 = p7 + dt * (-k.ay[i] * p7 - k.by[i] * dz);
-                rz += q7;
-                f7[ip] = q7;
+        for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
+            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            bool ok[kEpi], slab[kEpi];
+            float r2[kEpi], p7[kEpi];
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                const int t = t0 + u * blockDim.x;
+                ok[u] = t < n * P;
+                pu[u] = t % P;
+                iu[u] = t / P;
+                const int z = z0 + pu[u];
+                ipu[u] = cell(k, x, iu[u], z);
+                slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
+                r2[u] = ok[u] ? R2[ipu[u]] : 0.f;
+                p7[u] = slab[u] ? f7[ipu[u]] : 0.f;
             }
-            R2[ip] = rz;
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                if (!ok[u]) continue;
+                const int i = iu[u], ip = ipu[u];
+                const float dz = D[i * P + pu[u]];
+                float rz = r2[u] + dz;
+                if (slab[u]) {
+                    const float q7 = p7[u] + dt * (-k.ay[i] * p7[u] - k.by[i] * dz);
+                    rz += q7;
+                    f7[ip] = q7;
+                }
+                R2[ip] = rz;
+            }
         }
     }
 }
@@ -770,24 +804,45 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
             D[(n + i) * P + p] = v.y;
         };
         fft_any<N, 16, kThreads, kPencil, true>(k.px, tw, X1, Zf, P, 1, P, load_i, store_i);
-        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
-            const int p = t % P, i = t / P, z = z0 + p;
-            if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
-            const int ip = cell(k, i, y, z);
-            const bool slab = in_slab(i, nx, pml);
-            const float a0 = v0[ip], a1 = v1[ip], r0 = R0[ip], r1 = R1[ip], w0 = ri0[ip], w1 = ri1[ip];
-            const float p0 = slab ? f0[ip] : 0.f, p3 = slab ? f3[ip] : 0.f;
-            float px = D[i * P + p], py = D[(n + i) * P + p];
-            if (slab) {
-                const float q0 = p0 + dt * (-k.axh[i] * p0 - k.bxh[i] * px);
-                const float q3 = p3 + dt * (-k.ax[i] * p3 - k.bx[i] * py);
-                px += q0;
-                py += q3;
-                f0[ip] = q0;
-                f3[ip] = q3;
+        for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
+            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            bool ok[kEpi], slab[kEpi];
+            float a0[kEpi], a1[kEpi], r0[kEpi], r1[kEpi], w0[kEpi], w1[kEpi], p0[kEpi], p3[kEpi];
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                const int t = t0 + u * blockDim.x;
+                pu[u] = t % P;
+                iu[u] = t / P;
+                const int z = z0 + pu[u];
+                ok[u] = t < n * P && iu[u] < nx - 1 && yin && z < k.nz - 1;
+                ipu[u] = cell(k, iu[u], y, z);
+                slab[u] = ok[u] && in_slab(iu[u], nx, pml);
+                const int ip = ipu[u];
+                a0[u] = ok[u] ? v0[ip] : 0.f;
+                a1[u] = ok[u] ? v1[ip] : 0.f;
+                r0[u] = ok[u] ? R0[ip] : 0.f;
+                r1[u] = ok[u] ? R1[ip] : 0.f;
+                w0[u] = ok[u] ? ri0[ip] : 0.f;
+                w1[u] = ok[u] ? ri1[ip] : 0.f;
+                p0[u] = slab[u] ? f0[ip] : 0.f;
+                p3[u] = slab[u] ? f3[ip] : 0.f;
             }
-            v0[ip] = a0 + dt * w0 * (px + r0);
-            v1[ip] = a1 + dt * w1 * (py + r1);
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                if (!ok[u]) continue;
+                const int i = iu[u], p = pu[u], ip = ipu[u];
+                float px = D[i * P + p], py = D[(n + i) * P + p];
+                if (slab[u]) {
+                    const float q0 = p0[u] + dt * (-k.axh[i] * p0[u] - k.bxh[i] * px);
+                    const float q3 = p3[u] + dt * (-k.ax[i] * p3[u] - k.bx[i] * py);
+                    px += q0;
+                    py += q3;
+                    f0[ip] = q0;
+                    f3[ip] = q3;
+                }
+                v0[ip] = a0[u] + dt * w0[u] * (px + r0[u]);
+                v1[ip] = a1[u] + dt * w1[u] * (py + r1[u]);
+            }
         }
         __syncthreads();
     }
@@ -809,20 +864,36 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
             D[i * P + 2 * q + 1] = v.y;
         };
         fft_any<N, 8, kThreads, kPencil, true>(k.px, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
-        for (int t = threadIdx.x; t < n * P; t += blockDim.x) {
-            const int p = t % P, i = t / P, z = z0 + p;
-            if (!(i < nx - 1 && yin && z < k.nz - 1)) continue;
-            const int ip = cell(k, i, y, z);
-            const bool slab = in_slab(i, nx, pml);
-            const float a2 = v2[ip], r2 = R2[ip], w2 = ri2[ip];
-            const float p6 = slab ? f6[ip] : 0.f;
-            float pz = D[i * P + p];
-            if (slab) {
-                const float q6 = p6 + dt * (-k.ax[i] * p6 - k.bx[i] * pz);
-                pz += q6;
-                f6[ip] = q6;
+        for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
+            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            bool ok[kEpi], slab[kEpi];
+            float a2[kEpi], r2[kEpi], w2[kEpi], p6[kEpi];
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                const int t = t0 + u * blockDim.x;
+                pu[u] = t % P;
+                iu[u] = t / P;
+                const int z = z0 + pu[u];
+                ok[u] = t < n * P && iu[u] < nx - 1 && yin && z < k.nz - 1;
+                ipu[u] = cell(k, iu[u], y, z);
+                slab[u] = ok[u] && in_slab(iu[u], nx, pml);
+                a2[u] = ok[u] ? v2[ipu[u]] : 0.f;
+                r2[u] = ok[u] ? R2[ipu[u]] : 0.f;
+                w2[u] = ok[u] ? ri2[ipu[u]] : 0.f;
+                p6[u] = slab[u] ? f6[ipu[u]] : 0.f;
             }
-            v2[ip] = a2 + dt * w2 * (pz + r2);
+#pragma unroll
+            for (int u = 0; u < kEpi; ++u) {
+                if (!ok[u]) continue;
+                const int i = iu[u], ip = ipu[u];
+                float pz = D[i * P + pu[u]];
+                if (slab[u]) {
+                    const float q6 = p6[u] + dt * (-k.ax[i] * p6[u] - k.bx[i] * pz);
+                    pz += q6;
+                    f6[ip] = q6;
+                }
+                v2[ip] = a2[u] + dt * w2[u] * (pz + r2[u]);
+            }
         }
     }
 }
