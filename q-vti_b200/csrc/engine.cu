@@ -216,7 +216,7 @@ namespace {
 
 // Number of full-grid float arrays and half-spectrum complex arrays.
 constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 12 + 5 + 3;
-constexpr int kSpecArrays = 3 + 3 + kNumGxy;  // H, Hy, G without the kz-only fields
+constexpr int kSpecArrays = 3 + 3 + 3 + kNumGxy;  // H, Hy, Yv, G without the one-axis fields
 
 int build_graph(Sim* s)
 {
@@ -330,6 +330,10 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
         k.G[c] = nullptr;
         if (!is_gz(c)) rc |= s->alloc(&k.G[c], nspec);
     }
+    // the y derivatives live where the x/y pipeline would have put them
+    k.Yv[0] = k.G[16];  // dy vx
+    k.Yv[1] = k.G[4];   // dy vy
+    k.Yv[2] = k.G[25];  // dy vz
     rc |= s->alloc(&s->d_it, 1);
     rc |= s->alloc(&s->d_norm, 16);
     rc |= s->alloc(&s->d_bad, 4);
@@ -663,10 +667,10 @@ static void kernel_bytes(const qvti_sim* s, double* b)
     b[0] = 3 * F + 6 * F + 24 * cy;                                        // k_vy
     b[1] = 3 * F + 6 * F + 3 * F + 3 * F + 24 * cx;                        // k_vx
     b[2] = 3 * F + 3 * S;                                                  // k_fz
-    b[3] = 3 * 2 * S;                                                      // k_cy_fwd
+    b[3] = 3 * 3 * S;                                                      // k_cy_fwd (H -> Hy, Yv)
     b[4] = 3 * S + qvti::kNumGxy * S;                                      // k_mx
     b[5] = qvti::kNumGxy * 2 * S;                                          // k_cy_inv
-    // k_sigma: 27 half spectra (24 G, 3 H), 6 stresses and 6 loss potentials read+written,
+    // k_sigma: 27 half spectra (21 G, 3 H, 3 Yv), 6 stresses and 6 loss potentials read+written,
     // model + MU, 3 R written, C-PML variables in their slabs
     b[6] = qvti::kNumG * S + 12 * F + 12 * F + model + 5 * F + 3 * F + 3 * 8 * cz +
            (48 + 16 + 16) * cx + (48 + 16 + 16) * cy + (32 + 16 + 16) * cz;

@@ -21,10 +21,12 @@
 //              built once per shot in FP64 and rounded              float
 //   H[3]       velocity spectra, half along z: [kz][x][y], nkz = nz/2+1 float2
 //   Hy[3]      the same, transformed along y too: [kz][x][ky]       float2
+//   Yv[3]      dy vy, dy vx, dy vz with the identity dispersion operator,
+//              written by the forward y pass: [kz][x][y]            float2
 //   G[27]      9 directional derivatives x 3 dispersion operators
 //              (|k|^-1, 1, |k|) of the velocity spectra, [kz][x][y]; the
-//              three whose multiplier depends on kz alone (kGz) are not
-//              stored: k_sigma forms them from H                      float2
+//              six whose multiplier depends on kz or ky alone are not
+//              stored: k_sigma forms them from H and Yv               float2
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -34,13 +36,15 @@
 namespace qvti {
 
 constexpr int kNumG = 27;
-// G indices o = 3 d + j of the z derivatives with the identity dispersion
-// operator (d = 2 dz vz, 3 dz vx, 7 dz vy; j = 1): their multiplier
-// i kz e^{+-i kz dz/2} depends on kz alone, so IFFT3(M FFT3(v)) is a z
-// transform of H -- they skip the x and y passes.
-constexpr int kGz[3] = {7, 10, 22};
-constexpr int kNumGxy = kNumG - 3;  // fields that go through k_mx and k_cy
+// G indices o = 3 d + j of the z and y derivatives with the identity
+// dispersion operator (j = 1; d = 2 dz vz, 3 dz vx, 7 dz vy; d = 1 dy vy,
+// 5 dy vx, 8 dy vz): their multiplier i k e^{+-i k h/2} depends on one
+// wavenumber, so IFFT3(M FFT3(v)) needs only that axis' transform -- the z
+// ones are formed from H in k_sigma, the y ones in the forward y pass, and
+// neither goes through the x pass or the inverse y pass.
+constexpr int kNumGxy = kNumG - 6;  // fields that go through k_mx and k_cy
 __host__ __device__ constexpr bool is_gz(int o) { return o == 7 || o == 10 || o == 22; }
+__host__ __device__ constexpr bool is_gy(int o) { return o == 4 || o == 16 || o == 25; }
 
 struct KP {
     int nx, ny, nz, nkz, pml;
@@ -76,6 +80,7 @@ struct KP {
     // spectra
     float2* H[3];
     float2* Hy[3];
+    float2* Yv[3];  // null: the forward y pass writes no y derivative
     float2* G[kNumG];
     // source and receivers
     int src_type, s_ix, s_iy, s_iz;
@@ -99,7 +104,7 @@ struct StepProfile {
 void launch_step(const KP& kp, cudaStream_t st, StepProfile* prof = nullptr);
 // Largest dynamic shared memory (bytes) one of the step's launches needs.
 size_t step_smem_bytes(const KP& kp);
-constexpr size_t kMaxSmem = 227 * 1024;
+constexpr size_t kMaxSmem = 226 * 1024;  // dynamic; an SM block takes 227 KB with static
 // coef_out: 7 model arrays (rho gp gs c11 c33 c13 cs) then the 5 S-set arrays
 // (input of the MU average).
 void launch_coef_build(const KP& kp, const float* velp, const float* vels, const float* rho,

@@ -81,7 +81,7 @@ __constant__ int c_comp[9] = {0, 1, 2, 0, 2, 0, 1, 1, 2};
 __constant__ int c_axis[9] = {0, 1, 2, 2, 0, 1, 0, 2, 1};
 __constant__ int c_fwd[9] = {1, 1, 1, 0, 0, 0, 0, 0, 0};
 // G indices that go through the x and y passes (all but kGz)
-__constant__ int c_gxy[kNumGxy] = {0, 1, 2, 3, 4, 5, 6, 8, 9, 11, 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 23, 24, 25, 26};
+__constant__ int c_gxy[kNumGxy] = {0, 1, 2, 3, 5, 6, 8, 9, 11, 12, 13, 14, 15, 17, 18, 19, 20, 21, 23, 24, 26};
 
 // ------------------------------------------------------------------ k_fz --
 // R2C along z of vx, vy, vz.  Tile: one x, P consecutive y rows (P even);
@@ -135,16 +135,36 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     float2* tw = sm;
     float2* A = tw + n;
     float2* B = A + L * (n + n / 16);
+    float2* C = B + L * (n + n / 16);  // forward with Yv: the lines' y spectra, [L][n]
     load_table(tw, k.tw_y, n);
     __syncthreads();
     // forward: H -> Hy (H stays for k_sigma's kz-only fields); inverse: G in
     // place, blockIdx.y over the fields that went through k_mx
+    const int c = blockIdx.y;
     const long long off = (line0 + (long long)blockIdx.x * L) * n;
-    const float2* src = (INV ? k.G[c_gxy[blockIdx.y]] : k.H[blockIdx.y]) + off;
-    float2* dst = (INV ? k.G[c_gxy[blockIdx.y]] : k.Hy[blockIdx.y]) + off;
+    const float2* src = (INV ? k.G[c_gxy[c]] : k.H[c]) + off;
+    float2* dst = (INV ? k.G[c_gxy[c]] : k.Hy[c]) + off;
+    const bool ydv = !INV && k.Yv[c] != nullptr;
     auto load = [&](int p, int i) -> float2 { return src[(long long)p * n + i]; };
-    auto store = [&](int p, int i, float2 v) { dst[(long long)p * n + i] = v; };
+    auto store = [&](int p, int i, float2 v) {
+        dst[(long long)p * n + i] = v;
+        if (ydv) C[p * n + i] = v;
+    };
     fft_any<N, 8, kCyThreads, kLinePad, INV>(k.py, tw, A, B, L, n + n / 16, 1, load, store);
+    if constexpr (!INV) {
+        if (ydv) {
+            // the y derivative with the identity dispersion operator, scaled
+            // by 1/(ny nz) like a field of the x and y passes (1/ntp times
+            // the x round trip's nx): dy vy (c = 1, forward shift), dy vx and
+            // dy vz (backward)
+            const float2* T = c == 1 ? k.Fy : k.By;
+            const float inv_n = 1.0f / ((float)n * (float)k.nz);
+            float2* yd = k.Yv[c] + off;
+            auto load_d = [&](int p, int i) -> float2 { return cmul(C[p * n + i], cscale(T[i], inv_n)); };
+            auto store_d = [&](int p, int i, float2 v) { yd[(long long)p * n + i] = v; };
+            fft_any<N, 8, kCyThreads, kLinePad, true>(k.py, tw, A, B, L, n + n / 16, 1, load_d, store_d);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ k_mx --
@@ -198,7 +218,7 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
         if (c_comp[d] != c) continue;
         const int ax = c_axis[d], fw = c_fwd[d];
         for (int j = 0; j < 3; ++j) {
-            if (is_gz(3 * d + j)) continue;  // formed from H in k_sigma
+            if (is_gz(3 * d + j) || is_gy(3 * d + j)) continue;  // one-axis fields: formed elsewhere
             float2* G = k.G[3 * d + j];
             auto load = [&](int p, int i) -> float2 {
                 const float kyv = tky[p];
@@ -305,6 +325,15 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         ty[3 * P + i] = k.byh[y0 + i];
     }
     const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
+    // where each of the 27 fields comes from: G (x/y passes), Yv (forward y
+    // pass, already scaled) or H times the z shift multiplier (kind 1:
+    // forward, 2: backward)
+    __shared__ const float2* s_src[kNumG];
+    __shared__ int s_kind[kNumG];
+    for (int o = threadIdx.x; o < kNumG; o += blockDim.x) {
+        s_src[o] = is_gz(o) ? k.H[o == 7 ? 2 : o == 10 ? 0 : 1] : is_gy(o) ? k.Yv[o == 4 ? 1 : o == 16 ? 0 : 2] : k.G[o];
+        s_kind[o] = is_gz(o) ? (o == 7 ? 1 : 2) : 0;
+    }
     __syncthreads();
     const int it = *k.d_it;
     const float inv_nz = 1.0f / n;
@@ -344,17 +373,17 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
-        // a kz-only field (is_gz) is M(kz) H(kz) / nz: the same value the x
-        // and y round trip (normalised by 1/ntp) would have produced
+        // a kz-only field (is_gz) is M(kz) H(kz) / nz, a ky-only one (is_gy)
+        // Yv, which the forward y pass scaled alike: the values the x and y
+        // round trip (normalised by 1/ntp) would have produced
         auto load = [&](int pp, int i) -> float2 {
             const int f = pp / Qp, q = pp - f * Qp, o = o0 + f;
             const int kk = i <= n / 2 ? i : n - i;
-            const bool gz = is_gz(o);
-            const float2* src = gz ? k.H[o == 7 ? 2 : o == 10 ? 0 : 1] : k.G[o];
-            const float4 gg = *reinterpret_cast<const float4*>(src + spec(k, kk, x, y0 + 2 * q));
+            const float4 gg = *reinterpret_cast<const float4*>(s_src[o] + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
-            if (gz) {  // o == 7: forward shift (dz vz); 10, 22: backward
-                const float2 m = cscale(tzs[(o == 7 ? 0 : n) + kk], inv_nz);
+            const int kind = s_kind[o];
+            if (kind) {
+                const float2 m = cscale(tzs[(kind == 1 ? 0 : n) + kk], inv_nz);
                 a = cmul(a, m);
                 b = cmul(b, m);
             }
@@ -1108,7 +1137,10 @@ int tile_of(int n, int want)
 }
 
 size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + k.nz / 16)); }
-size_t smem_cy(const KP& k, int L) { return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16)); }
+size_t smem_cy(const KP& k, int L, bool ydv = false)
+{
+    return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16) + (ydv ? (size_t)L * k.ny : 0));
+}
 size_t smem_mx(const KP& k, int P)
 {
     const int nbuf = k.px.nst > 2 ? 2 : 1;
@@ -1158,7 +1190,7 @@ constexpr int kCtLengths[] = {0, 64, 96, 128, 144, 160, 192, 240, 256, 288, 320,
 
 int configure_kernels()
 {
-    const int big = 227 * 1024;
+    const int big = (int)kMaxSmem;  // leaves room for the kernels' small static tables
     cudaError_t e = cudaSuccess;
     auto set = [&](const void* f) {
         cudaError_t r = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
@@ -1220,7 +1252,8 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
         const long long line0 = (long long)kz0 * k.nx;
         dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L), st>>>(k, L, line0);
+            k_cy<decltype(NN)::value, false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L,
+                                                                                                             line0);
         });
         mark(3);
         dispatch_len(len(k.nx, Pm, 16), [&](auto NN) {
@@ -1253,7 +1286,7 @@ size_t step_smem_bytes(const KP& k)
     size_t m = smem_vyx(k.ny, Pv);
     m = std::max(m, smem_vyx(k.nx, Pv));
     m = std::max(m, smem_fz(k, Pz));
-    m = std::max(m, smem_cy(k, L));
+    m = std::max(m, smem_cy(k, L, true));
     m = std::max(m, smem_mx(k, Pm));
     m = std::max(m, smem_sigma(k, Ps, false));  // the larger layout
     return m;
@@ -1280,6 +1313,7 @@ void launch_q_derivative(const KP& k_in, int axis, int fwd, int pw, float* out, 
 {
     KP k = k_in;
     k.Hy[0] = k.H[0];  // the forward y pass works in place on the one scratch spectrum
+    for (int c = 0; c < 3; ++c) k.Yv[c] = nullptr;  // and writes no y derivative
     const int Pz = tile_of(k.ny, 16);
     k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
     const int L = tile_of(k.nx, 8);
