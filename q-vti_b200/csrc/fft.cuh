@@ -380,7 +380,7 @@ struct FftCT {
         else return p * (N + 1) + i;
     }
 
-    template <int S, bool INV, bool CHAIN = true, class Load, class Store>
+    template <int S, bool INV, class Load, class Store>
     static __device__ __forceinline__ void stage(const float2* __restrict__ tw, float2* A, float2* B, Load& load,
                                                  Store& store)
     {
@@ -441,7 +441,7 @@ struct FftCT {
             }
         }
         __syncthreads();
-        if constexpr (!LAST && CHAIN) stage<S + 1, INV>(tw, A, B, load, store);
+        if constexpr (!LAST) stage<S + 1, INV>(tw, A, B, load, store);
     }
 
     // Stage 0 reads `load`, the last stage writes `store`; ends with
@@ -455,54 +455,6 @@ struct FftCT {
 
     // The buffer the last stage does not read.
     static __device__ __forceinline__ float2* out_buf(float2* A, float2* B) { return ((NST - 1) & 1) ? B : A; }
-
-    // Two-stage transform whose output may overwrite its own staging buffer A
-    // (the store functor writes into A's memory): every thread holds one
-    // last-stage task, reads and transforms it in registers, and stores only
-    // after the whole block has read A.  Ends with __syncthreads().
-    template <bool INV, class Load, class Store>
-    static __device__ __forceinline__ void run_inplace(const float2* __restrict__ tw, float2* A, Load load,
-                                                       Store store)
-    {
-        static_assert(NST == 2, "in-place last stage: two-stage lengths only");
-        constexpr int R = ct_rad(N, 1), NS = ct_ns(N, 1);
-        constexpr int NR = N / R, TOTAL = P * NR, TWS = N / (NS * R);
-        static_assert(TOTAL <= NT, "in-place last stage: at most one task per thread");
-        auto none = [](int, int, float2) {};
-        stage<0, INV, false>(tw, A, A, load, none);
-        const int t = threadIdx.x;
-        const bool act = t < TOTAL;
-        float2 v[R];
-        int p = 0, j = 0, jm = 0;
-        if (act) {
-            if (PF) { p = t % P; j = t / P; }
-            else    { j = t % NR; p = t / NR; }
-            jm = j % NS;
-            if constexpr (LY != kLine && NR % 16 == 0) {
-                const int b = at(p, j);
-#pragma unroll
-                for (int r = 0; r < R; ++r) v[r] = A[b + r * (NR + NR / 16) * PSTEP];
-            } else {
-#pragma unroll
-                for (int r = 0; r < R; ++r) v[r] = A[at(p, j + r * NR)];
-            }
-            if (jm) {
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const float2 w = tw[jm * r * TWS];
-                    v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
-                }
-            }
-            Dft<R>::run(v, INV);
-        }
-        __syncthreads();  // A has been read in full: outputs may overwrite it
-        if (act) {
-            const int base = (j - jm) * R + jm;
-#pragma unroll
-            for (int r = 0; r < R; ++r) store(p, base + r * NS, v[r]);
-        }
-        __syncthreads();
-    }
 };
 
 }  // namespace qvti

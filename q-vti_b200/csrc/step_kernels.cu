@@ -255,10 +255,11 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 }
 
 constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
-// A two-stage compile-time length runs its C2R with the in-place last stage
-// (the real field tile S overwrites the staging buffer A) on 288 threads: 9
-// fields x 2 pencils x 16 radix-16 butterflies, one task per thread.  That
-// drops S's own 37 KB (256 points), so three blocks fit an SM instead of two.
+// A two-stage compile-time length keeps the C2R's real fields in its staging
+// buffer A (the last stage writes each result into the slot it read, see
+// k_sigma) on 288 threads: 9 fields x 2 pencils x 16 radix-16 butterflies,
+// one task per thread.  That drops a separate 37 KB real tile (256 points),
+// so three blocks fit an SM instead of two.
 constexpr bool sigma_inplace(int n) { return n > 0 && ct_nst(n) == 2; }
 constexpr int sigma_threads(int n) { return sigma_inplace(n) ? 9 * kSigmaRows / 2 * 16 : kThreads; }
 constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
@@ -397,13 +398,37 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             S[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
         if constexpr (INPLACE) {
-            if (grp == 0) FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>::template run_inplace<true>(tw, A, load, store);
-            else FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>::template run_inplace<true>(tw, A, load, store);
+            // The last Stockham stage's butterfly writes exactly the indices
+            // it read (j + r N/R), so each pencil pair's real rows go back,
+            // as one float2, into the slot of the staging tile they came from:
+            // every thread overwrites only its own inputs, no barrier or
+            // register staging needed.  The update reads them through sval.
+            if (grp == 0) {
+                using F = FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>;
+                auto keep = [&](int pp, int i, float2 v) { A[F::at(pp, i)] = v; };
+                F::template run<true>(tw, A, A, load, keep);
+            } else {
+                using F = FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>;
+                auto keep = [&](int pp, int i, float2 v) { A[F::at(pp, i)] = v; };
+                F::template run<true>(tw, A, A, load, keep);
+            }
         } else {
             if (grp == 0) fft_any<N, 9 * kSigmaRows / 2, NT, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
             else fft_any<N, 6 * kSigmaRows / 2, NT, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
         }
 
+        // real value of field f (of this group), row p, height z
+        const float* Af = reinterpret_cast<const float*>(A);
+        auto sval = [&](int f, int p, int z) -> float {
+            if constexpr (INPLACE) {
+                const int pp = f * Qp + (p >> 1);
+                const int slot = grp == 0 ? FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>::at(pp, z)
+                                          : FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>::at(pp, z);
+                return Af[2 * slot + (p & 1)];
+            } else {
+                return S[(f * P + p) * np1 + z];
+            }
+        };
         // 2. stress update of the group.  Each thread owns kCells cells; all
         //    their streaming inputs are loaded before any store so the loads
         //    are in flight together (the arrays cannot alias, but the
@@ -442,7 +467,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                     const int p = t / n, z = t - p * n, y = y0 + p;
                     const int ip = ipv[u];
                     const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
-                    auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
+                    auto sv = [&](int f) { return sval(f, p, z); };
                     float sxx = in[u][0], syy = in[u][1], szz = in[u][2];
                     if (upd) {
                         float a11[5], a33[5], a13[5], s5[5], a12[5];
@@ -547,7 +572,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                     const int p = t / n, z = t - p * n, y = y0 + p;
                     const int ip = ipv[u];
                     const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
-                    auto sv = [&](int f) { return S[(f * P + p) * np1 + z]; };
+                    auto sv = [&](int f) { return sval(f, p, z); };
                     float sig = in[u][0];
                     if (upd) {
                         const float* mu = &in[u][2];
