@@ -255,17 +255,17 @@ __device__ __forceinline__ void qset_f(float rho, float c, float g, float w0, fl
 }
 
 constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
-// A two-stage compile-time length keeps the C2R's real fields in its staging
-// buffer A (the last stage writes each result into the slot it read, see
+// A compile-time length keeps the C2R's real fields in the buffer its last
+// stage reads (that stage writes each result into the slot it read, see
 // k_sigma) on 288 threads: 9 fields x 2 pencils x 16 radix-16 butterflies,
-// one task per thread.  That drops a separate 37 KB real tile (256 points),
-// so three blocks fit an SM instead of two.
-constexpr bool sigma_inplace(int n) { return n > 0 && ct_nst(n) == 2; }
+// one task per thread in a radix-16 stage.  That drops a separate real tile
+// (37 KB at 256 points, so three blocks fit an SM instead of two).
+constexpr bool sigma_inplace(int n) { return n > 0; }
 constexpr int sigma_threads(int n) { return sigma_inplace(n) ? 9 * kSigmaRows / 2 * 16 : kThreads; }
 constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
 {
     const size_t bufA = (size_t)9 * (kSigmaRows / 2) * (n + n / 16);  // float2
-    const size_t nb = sigma_inplace(n) ? 1 : (ct_nst(n) > 2 ? 2 : 1);
+    const size_t nb = ct_nst(n) > 2 ? 2 : 1;
     const size_t sreal = sigma_inplace(n) ? 0 : (size_t)9 * kSigmaRows * (n + 1);
     return 8 * ((size_t)n + nb * bufA + 2 * (size_t)n) +
            4 * (sreal + (size_t)3 * kSigmaRows * (n + 1) + 4 * (size_t)n + 4 * kSigmaRows);
@@ -304,8 +304,11 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     // there is no B (the z-derivative pass uses D as its second buffer);
     // otherwise B aliases S when the transform has two stages.
     float2* B = A + bufA;
-    float* S = INPLACE ? reinterpret_cast<float*>(A) : reinterpret_cast<float*>(B + (two_buf ? bufA : 0));
-    float* D = INPLACE ? reinterpret_cast<float*>(A + bufA) : S + 9 * P * np1;  // [3][P][np1]: szz sxz syz
+    // the buffer the C2R's last stage reads: with the results written back in
+    // place, the group's real fields live there
+    float2* Lb = (N > 0 && ((ct_nst(N) - 2) & 1)) ? B : A;
+    float* S = reinterpret_cast<float*>(B + (two_buf ? bufA : 0));  // not used in place
+    float* D = INPLACE ? S : S + 9 * P * np1;                         // [3][P][np1]: szz sxz syz
     float* tz = D + 3 * P * np1;                                          // [4][n]: az bz azh bzh
     float* ty = tz + 4 * n;                                               // [4][P]: ay by ayh byh of the rows
     float2* tzs = reinterpret_cast<float2*>(ty + 4 * P);                  // [2][n]: Fz Bz
@@ -405,12 +408,12 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             // register staging needed.  The update reads them through sval.
             if (grp == 0) {
                 using F = FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>;
-                auto keep = [&](int pp, int i, float2 v) { A[F::at(pp, i)] = v; };
-                F::template run<true>(tw, A, A, load, keep);
+                auto keep = [&](int pp, int i, float2 v) { Lb[F::at(pp, i)] = v; };
+                F::template run<true>(tw, A, B, load, keep);
             } else {
                 using F = FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>;
-                auto keep = [&](int pp, int i, float2 v) { A[F::at(pp, i)] = v; };
-                F::template run<true>(tw, A, A, load, keep);
+                auto keep = [&](int pp, int i, float2 v) { Lb[F::at(pp, i)] = v; };
+                F::template run<true>(tw, A, B, load, keep);
             }
         } else {
             if (grp == 0) fft_any<N, 9 * kSigmaRows / 2, NT, kPencil, true>(k.pz, tw, A, B, npen, 1, npen, load, store);
@@ -418,7 +421,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         }
 
         // real value of field f (of this group), row p, height z
-        const float* Af = reinterpret_cast<const float*>(A);
+        const float* Af = reinterpret_cast<const float*>(Lb);
         auto sval = [&](int f, int p, int z) -> float {
             if constexpr (INPLACE) {
                 const int pp = f * Qp + (p >> 1);
@@ -617,7 +620,9 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             const int f = pp / Qp, q = pp - f * Qp;
             return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
         };
-        float2* B2 = INPLACE ? reinterpret_cast<float2*>(D) : B;  // D is read only by stage 0
+        // in place with two stages there is no B: D serves (it is read only by
+        // stage 0)
+        float2* B2 = (INPLACE && !two_buf) ? reinterpret_cast<float2*>(D) : B;
         float2* Zf = out_any<N, 3 * kSigmaRows / 2, NT, kLinePad>(k.pz, A, B2);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
         fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, false>(k.pz, tw, A, B2, npen, n + n / 16, 1, load, store_f);
@@ -1174,11 +1179,12 @@ size_t smem_mx(const KP& k, int P)
 // k_sigma layout: tw[nz] | A | B (only when the z transform has more than two
 // stages; otherwise B aliases S, used only by the final z-derivative pass) |
 // S[9][P][nz+1] | D[3][P][nz+1] | z tables [4][nz] | y tables [4][P] | Fz, Bz.
-// In place (two-stage compile-time lengths): tw | A (= S) | D | tables.
+// In place (compile-time lengths): tw | A | B (more than two stages) | D |
+// tables; the real fields live in the buffer the last C2R stage reads.
 size_t smem_sigma(const KP& k, int P, bool inplace)
 {
     const size_t bufA = (size_t)9 * (P / 2) * (k.nz + k.nz / 16);
-    const int nb = inplace ? 1 : (k.pz.nst > 2 ? 2 : 1);
+    const int nb = k.pz.nst > 2 ? 2 : 1;
     const size_t sreal = inplace ? 0 : (size_t)9 * P * (k.nz + 1);
     return sizeof(float2) * (k.nz + nb * bufA + 2 * k.nz) +
            sizeof(float) * (sreal + (size_t)3 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
