@@ -1194,8 +1194,8 @@ size_t smem_vyx(int n, int P) { return sizeof(float2) * (2 * n + 2 * (n + n / 16
 
 }  // namespace
 
-// Transform lengths with a compile-time path (the multiples of 16 among the
-// grids the batching and serving workloads draw, and the common cubes); a
+// Transform lengths with a compile-time path (the even 5-smooth sizes the
+// batching and serving workloads draw between 96 and 384, and 64 and 512); a
 // kernel takes it when its transform length is listed and its tile fits the
 // grid (see launch_step), otherwise the runtime path.
 template <class F>
@@ -1204,20 +1204,33 @@ void dispatch_len(int n, F&& f)
     switch (n) {
         case 64: f(std::integral_constant<int, 64>{}); break;
         case 96: f(std::integral_constant<int, 96>{}); break;
+        case 100: f(std::integral_constant<int, 100>{}); break;
+        case 108: f(std::integral_constant<int, 108>{}); break;
+        case 120: f(std::integral_constant<int, 120>{}); break;
         case 128: f(std::integral_constant<int, 128>{}); break;
         case 144: f(std::integral_constant<int, 144>{}); break;
+        case 150: f(std::integral_constant<int, 150>{}); break;
         case 160: f(std::integral_constant<int, 160>{}); break;
+        case 162: f(std::integral_constant<int, 162>{}); break;
+        case 180: f(std::integral_constant<int, 180>{}); break;
         case 192: f(std::integral_constant<int, 192>{}); break;
+        case 200: f(std::integral_constant<int, 200>{}); break;
+        case 216: f(std::integral_constant<int, 216>{}); break;
         case 240: f(std::integral_constant<int, 240>{}); break;
+        case 250: f(std::integral_constant<int, 250>{}); break;
         case 256: f(std::integral_constant<int, 256>{}); break;
+        case 270: f(std::integral_constant<int, 270>{}); break;
         case 288: f(std::integral_constant<int, 288>{}); break;
+        case 300: f(std::integral_constant<int, 300>{}); break;
         case 320: f(std::integral_constant<int, 320>{}); break;
+        case 324: f(std::integral_constant<int, 324>{}); break;
+        case 360: f(std::integral_constant<int, 360>{}); break;
         case 384: f(std::integral_constant<int, 384>{}); break;
         case 512: f(std::integral_constant<int, 512>{}); break;
         default: f(std::integral_constant<int, 0>{}); break;
     }
 }
-constexpr int kCtLengths[] = {0, 64, 96, 128, 144, 160, 192, 240, 256, 288, 320, 384, 512};
+constexpr int kCtLengths[] = {0, 64, 96, 100, 108, 120, 128, 144, 150, 160, 162, 180, 192, 200, 216, 240, 250, 256, 270, 288, 300, 320, 324, 360, 384, 512};
 
 int configure_kernels()
 {

@@ -96,12 +96,14 @@ def test_explosive_source_against_oracle(qvti, oracle):
     _compare(ours, ref, "explosive")
 
 
-@pytest.mark.parametrize("n", [(64, 64, 64), (64, 128, 96), (160, 32, 48), (48, 144, 32), (32, 48, 192)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (64, 128, 96), (160, 32, 48), (48, 144, 32), (32, 48, 192),
+                               (120, 32, 48), (32, 108, 48), (40, 48, 100)])
 def test_compile_time_path_against_oracle(qvti, oracle, n):
     """A kernel takes the compile-time FFT path when its transform length is
     compiled and its tile fits the grid; the mixed grids put some kernels on
-    it (x: k_vx, k_mx at 160; y: k_vy, k_cy at 144; z: k_fz, k_sigma at the
-    three-stage 192) and the rest on the runtime path.  VTI, heterogeneous,
+    it (x: k_vx, k_mx at 160 and 120; y: k_vy, k_cy at 144 and 108; z: k_fz,
+    k_sigma at the three-stage 192 and at 100) and the rest on the runtime
+    path.  VTI, heterogeneous,
     receivers 6 cells above and within 3 cells of the source."""
     nt = 100 if n[0] * n[1] * n[2] <= 64 ** 3 else 80
     c = qc.heterogeneous_case(n=n, pml=8, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=nt, f0=30.0, seed=21,
