@@ -78,3 +78,11 @@ def test_reference_harness_exports():
     for n in ("qref_run", "cuda_forward_acoustic_3D", "cuda_Device_malloc", "cuda_Device_free",
               "cuda_Host_initialization", "getdevice"):
         assert hasattr(lib, n)
+
+
+def test_host_driver_builds(qvti):
+    """The C++ host driver with the reference's host surface compiles and
+    links against the library (no GPU needed)."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "q-vti_b200"), "driver"])
+    assert os.access(os.path.join(ROOT, "q-vti_b200", "qvti_driver"), os.X_OK)
