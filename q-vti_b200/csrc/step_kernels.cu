@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
                 const float kxv = tkx[i];
                 float k2 = kxv * kxv + kyv * kyv + kz2;
                 k2 = fmaxf(k2, 1e-10f);  // the reference sets |k|^2 = 1e-10 at DC (cu:74)
-                const float ap = j == 1 ? 1.0f : (j == 0 ? 1.0f / sqrtf(k2) : sqrtf(k2));
+                // |k|^-1 and |k| from the hardware reciprocal square root
+                // (~2 ulp): far below the FP32 transforms' own rounding
+                const float rk = rsqrtf(k2);
+                const float ap = j == 1 ? 1.0f : (j == 0 ? rk : k2 * rk);
                 float2 T;
                 if (ax == 0) T = fw ? tFx[i] : tBx[i];
                 else if (ax == 1) T = fw ? tFBy[p] : tFBy[P + p];
