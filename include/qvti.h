@@ -115,6 +115,28 @@ int qvti_device_field(qvti_sim* sim, int which, float** dev_ptr);
  * per-run energy-norm check; also flags non-finite values. */
 int qvti_field_norms(qvti_sim* sim, double* norms9, int* nonfinite);
 
+/* Checkpoint / resume.  A snapshot holds everything a step reads that an
+ * earlier step wrote: particle velocities, stresses, the z-derivative
+ * accumulators carried into the next velocity update, the loss potentials
+ * and the C-PML memory variables (55 full-grid arrays), the step count and
+ * the seismograms recorded so far.  The model, source wavelet and receivers
+ * are inputs, not state: set them on the resuming simulation as for the
+ * original run (the reference declares checkpoint variables but never uses
+ * them, viscoelas_3D.cpp:223-229).  Resuming is bitwise: steps run after
+ * qvti_load_state give exactly the records and wavefields of an
+ * uninterrupted run.
+ *
+ * qvti_state_bytes: size of a snapshot of this simulation at its current
+ * step.  qvti_save_state: copies the snapshot into `host` (at least that
+ * many bytes), after the simulation's queued steps.  qvti_load_state:
+ * restores a snapshot; QVTI_ERR_ARG if the buffer is not a snapshot, or was
+ * taken on another grid, spacing, dt, C-PML width or medium type, or holds
+ * more recorded steps or another receiver count than this simulation's
+ * source and receivers allow; QVTI_ERR_STATE before a source is set. */
+int qvti_state_bytes(qvti_sim* sim, size_t* bytes);
+int qvti_save_state(qvti_sim* sim, void* host, size_t bytes);
+int qvti_load_state(qvti_sim* sim, const void* host, size_t bytes);
+
 /* One whole shot with host buffers, synchronous: model upload, setup,
  * nt steps, seismogram download.  The reference-call semantics of
  * cuda_forward_acoustic_3D (Myfunctions.h:77-85, cuviscoelas_3D.cu:1137-1652)

@@ -1,6 +1,7 @@
 // Host side of the engine: allocation, FP64 setup on the GPU, CUDA-graph
 // replay of the step, and the qvti_* C ABI (include/qvti.h).
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -618,6 +619,132 @@ extern "C" int qvti_field_norms(qvti_sim* s, double* norms9, int* nonfinite)
     }
     if (nonfinite) *nonfinite = bad_all;
     return bad_all ? fail(QVTI_ERR_NONFINITE) : QVTI_OK;
+}
+
+// ------------------------------------------------------ checkpoint / resume --
+namespace {
+
+// Snapshot layout: this header, then kStateArrays full-grid float arrays in
+// state_arrays() order, then the records of the steps done (vx, vy, vz, each
+// [step][receiver]).  Grid, spacing, dt, C-PML width and medium type are in
+// the header so a snapshot cannot resume a different simulation.
+struct StateHeader {
+    char magic[8];
+    int32_t ntx, nty, ntz, pml;
+    int32_t vti, n_arrays, steps, rn;
+    float dx, dy, dz, dt;
+    uint64_t array_bytes, total_bytes;
+};
+static_assert(sizeof(StateHeader) == 72, "snapshot header layout");
+constexpr char kStateMagic[8] = {'Q', 'V', 'T', 'I', 'S', 'T', '0', '1'};
+constexpr int kStateArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6;
+
+int state_arrays(Sim* s, float** out)
+{
+    qvti::KP& k = s->kp;
+    int n = 0;
+    for (float* p : k.v) out[n++] = p;
+    for (float* p : k.s) out[n++] = p;
+    for (float* p : k.R) out[n++] = p;
+    for (float* p : k.Q) out[n++] = p;
+    for (float* p : k.php) out[n++] = p;
+    for (float* p : k.phn) out[n++] = p;
+    for (float* p : k.qn) out[n++] = p;
+    for (float* p : k.phs) out[n++] = p;
+    for (float* p : k.qs) out[n++] = p;
+    return n;
+}
+
+StateHeader state_header(const Sim* s)
+{
+    StateHeader h{};
+    memcpy(h.magic, kStateMagic, sizeof(h.magic));
+    h.ntx = s->nx; h.nty = s->ny; h.ntz = s->nz; h.pml = s->cfg.pml;
+    h.vti = s->cfg.vti ? 1 : 0;
+    h.n_arrays = kStateArrays;
+    h.steps = s->steps;
+    h.rn = s->rn;
+    h.dx = s->cfg.dx; h.dy = s->cfg.dy; h.dz = s->cfg.dz; h.dt = s->cfg.dt;
+    h.array_bytes = sizeof(float) * (uint64_t)s->ntp;
+    const uint64_t rec = s->rn > 0 && s->d_rec[0] ? 3ull * s->steps * s->rn * sizeof(float) : 0;
+    h.total_bytes = sizeof(StateHeader) + h.array_bytes * kStateArrays + rec;
+    return h;
+}
+
+}  // namespace
+
+extern "C" int qvti_state_bytes(qvti_sim* s, size_t* bytes)
+{
+    if (!s || !bytes) return fail(QVTI_ERR_ARG);
+    *bytes = (size_t)state_header(s).total_bytes;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_save_state(qvti_sim* s, void* host, size_t bytes)
+{
+    using namespace qvti;
+    if (!s || !host) return fail(QVTI_ERR_ARG);
+    const StateHeader h = state_header(s);
+    if (bytes < h.total_bytes) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    char* dst = static_cast<char*>(host);
+    memcpy(dst, &h, sizeof(h));
+    dst += sizeof(h);
+    float* arr[kStateArrays];
+    state_arrays(s, arr);
+    for (float* p : arr) {
+        QV_CUDA(cudaMemcpyAsync(dst, p, h.array_bytes, cudaMemcpyDeviceToHost, s->st));
+        dst += h.array_bytes;
+    }
+    const size_t rec = sizeof(float) * (size_t)h.steps * h.rn;
+    if (h.total_bytes > sizeof(h) + h.array_bytes * kStateArrays)
+        for (int c = 0; c < 3; ++c) {
+            QV_CUDA(cudaMemcpyAsync(dst, s->d_rec[c], rec, cudaMemcpyDeviceToHost, s->st));
+            dst += rec;
+        }
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    return QVTI_OK;
+}
+
+extern "C" int qvti_load_state(qvti_sim* s, const void* host, size_t bytes)
+{
+    using namespace qvti;
+    if (!s || !host || bytes < sizeof(StateHeader)) return fail(QVTI_ERR_ARG);
+    if (!s->have_src) return fail(QVTI_ERR_STATE);
+    StateHeader h;
+    memcpy(&h, host, sizeof(h));
+    const StateHeader mine = state_header(s);
+    const bool same = memcmp(h.magic, kStateMagic, sizeof(h.magic)) == 0 && h.ntx == mine.ntx &&
+                      h.nty == mine.nty && h.ntz == mine.ntz && h.pml == mine.pml && h.vti == mine.vti &&
+                      h.n_arrays == kStateArrays && h.array_bytes == mine.array_bytes &&
+                      memcmp(&h.dx, &mine.dx, 4 * sizeof(float)) == 0;
+    if (!same || h.steps < 0 || h.steps > s->nt || h.rn != s->rn) return fail(QVTI_ERR_ARG);
+    const uint64_t rec = sizeof(float) * (uint64_t)h.steps * h.rn;
+    const bool with_rec = h.rn > 0 && s->d_rec[0];
+    const uint64_t want = sizeof(h) + h.array_bytes * kStateArrays + (with_rec ? 3 * rec : 0);
+    if (h.total_bytes != want || bytes < want) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    const char* src = static_cast<const char*>(host) + sizeof(h);
+    float* arr[kStateArrays];
+    state_arrays(s, arr);
+    for (float* p : arr) {
+        QV_CUDA(cudaMemcpyAsync(p, src, h.array_bytes, cudaMemcpyHostToDevice, s->st));
+        src += h.array_bytes;
+    }
+    if (with_rec) {
+        const size_t all = sizeof(float) * (size_t)s->nt * s->rn;
+        for (int c = 0; c < 3; ++c) {
+            QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, all, s->st));
+            if (rec) QV_CUDA(cudaMemcpyAsync(s->d_rec[c], src, rec, cudaMemcpyHostToDevice, s->st));
+            src += rec;
+        }
+    }
+    // the step kernels advance the counter first: after n steps it holds n - 1
+    const int it = h.steps - 1;
+    QV_CUDA(cudaMemcpyAsync(s->d_it, &it, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    s->steps = h.steps;
+    return QVTI_OK;
 }
 
 extern "C" int qvti_forward_shot(qvti_sim* s, const float* velp, const float* vels, const float* rho,

@@ -88,6 +88,9 @@ def lib():
             "qvti_get_fields": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _F]),
             "qvti_device_field": (ctypes.c_int, [_V, ctypes.c_int, ctypes.POINTER(_F)]),
             "qvti_field_norms": (ctypes.c_int, [_V, _D, _I]),
+            "qvti_state_bytes": (ctypes.c_int, [_V, ctypes.POINTER(ctypes.c_size_t)]),
+            "qvti_save_state": (ctypes.c_int, [_V, _V, ctypes.c_size_t]),
+            "qvti_load_state": (ctypes.c_int, [_V, _V, ctypes.c_size_t]),
             "qvti_forward_shot": (ctypes.c_int, [_V, _F, _F, _F, _F, _F, _F, _F, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int, _I,
                                                  _I, ctypes.c_int, _F, _F, _F]),
@@ -237,6 +240,19 @@ class Simulation:
         bad = ctypes.c_int(0)
         rc = lib().qvti_field_norms(self._h, out.ctypes.data_as(_D), ctypes.byref(bad))
         return out, bool(bad.value), rc
+
+    def save_state(self):
+        """Snapshot of the time-stepping state (qvti_save_state) as a uint8 array."""
+        n = ctypes.c_size_t(0)
+        _check(lib().qvti_state_bytes(self._h, ctypes.byref(n)), "qvti_state_bytes")
+        buf = np.empty(n.value, np.uint8)
+        _check(lib().qvti_save_state(self._h, buf.ctypes.data_as(_V), buf.size), "qvti_save_state")
+        return buf
+
+    def load_state(self, buf):
+        """Resume from a snapshot taken by save_state (after set_source/set_receivers)."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        _check(lib().qvti_load_state(self._h, b.ctypes.data_as(_V), b.size), "qvti_load_state")
 
     def profile_step(self, nrep=3):
         """Per-kernel device time of one step: list of (name, ms, algorithmic bytes)."""
