@@ -365,13 +365,24 @@ __host__ __device__ constexpr int ct_ns(int n, int stage)
 // free of bank conflicts.
 constexpr int kLine = 0, kPencil = 1, kLinePad = 2;
 
-template <int N, int P, int NT, int LY>
+// PRETW (two-stage transforms only): stage 0 multiplies its outputs by the
+// twiddles stage 1 would apply to them, so stage 1 starts its butterflies
+// straight from shared memory.  The products are the same, on the same
+// values; what changes is where they are computed: after stage 0's loads are
+// consumed, instead of with 16 values and 15 twiddles live in stage 1 (which
+// at 256 points spills under a 72-register cap).
+// ROLL: a stage of several butterfly rounds per thread (small radices, many
+// pencils) stays a loop instead of being unrolled, so the compiler does not
+// hoist every round's loads at once; for a kernel already near its register
+// cap that is the difference between spilling and not.
+template <int N, int P, int NT, int LY, bool PRETW = false, bool ROLL = false>
 struct FftCT {
     static constexpr bool PF = LY == kPencil;
     static constexpr int NST = ct_nst(N);
     static constexpr int BUF = LY == kLine ? P * (N + 1) : P * (N + N / 16);  // float2 per buffer
 
     static constexpr int PSTEP = LY == kPencil ? P : 1;  // distance of consecutive indices
+    static_assert(!PRETW || NST == 2, "stage-1 twiddles move into stage 0 only for two-stage transforms");
 
     static __device__ __forceinline__ int at(int p, int i)
     {
@@ -389,8 +400,10 @@ struct FftCT {
         constexpr int NR = N / R, TOTAL = P * NR, TWS = N / (NS * R);
         const float2* src = ((S - 1) & 1) ? B : A;
         float2* dst = (S & 1) ? B : A;
-#pragma unroll
-        for (int it = 0; it < (TOTAL + NT - 1) / NT; ++it) {
+        constexpr int ITER = (TOTAL + NT - 1) / NT;
+        constexpr int UNR = ROLL ? 1 : ITER;
+#pragma unroll(UNR)
+        for (int it = 0; it < ITER; ++it) {
             const int t = threadIdx.x + it * NT;
             if ((TOTAL % NT) != 0 && t >= TOTAL) break;
             int p, j;
@@ -410,7 +423,7 @@ struct FftCT {
 #pragma unroll
                 for (int r = 0; r < R; ++r) v[r] = src[at(p, j + r * NR)];
             }
-            if constexpr (!FIRST) {
+            if constexpr (!FIRST && !PRETW) {
                 if (jm) {
 #pragma unroll
                     for (int r = 1; r < R; ++r) {
@@ -420,6 +433,19 @@ struct FftCT {
                 }
             }
             Dft<R>::run(v, INV);
+            if constexpr (PRETW && FIRST) {
+                // two stages (NS = 1 here, R0 = NS of stage 1, TWS of stage 1
+                // = 1): output r of butterfly j lands at index j R + r, which
+                // stage 1 reads as its butterfly r, element j, with twiddle
+                // w^(r j)
+                if (j) {
+#pragma unroll
+                    for (int r = 1; r < R; ++r) {
+                        const float2 w = tw[r * j];
+                        v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
+                    }
+                }
+            }
             const int base = (j - jm) * R + jm;
             if constexpr (LAST) {
 #pragma unroll

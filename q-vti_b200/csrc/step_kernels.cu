@@ -58,11 +58,11 @@ __device__ __forceinline__ void load_table(float2* s, const float2* g, int n)
 // layout ps_rt/is_rt).  LY is the shared-memory layout (kLine, kPencil,
 // kLinePad); the padded layouts carry one padding row every 16 indices in
 // both paths.
-template <int N, int PC, int NT, int LY, bool INV, class Load, class Store>
+template <int N, int PC, int NT, int LY, bool INV, bool ROLL = false, class Load, class Store>
 __device__ __forceinline__ void fft_any(const FftPlan& pl, const float2* tw, float2* A, float2* B, int prt, int ps_rt,
                                         int is_rt, Load load, Store store)
 {
-    if constexpr (N > 0) FftCT<N, PC, NT, LY>::template run<INV>(tw, A, B, load, store);
+    if constexpr (N > 0) FftCT<N, PC, NT, LY, false, ROLL>::template run<INV>(tw, A, B, load, store);
     else fft_run<LY == kPencil>(pl, tw, A, B, prt, ps_rt, is_rt, INV, load, store, LY == kLine ? 0 : 4);
 }
 template <int N, int PC, int NT, int LY>
@@ -99,9 +99,11 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
     load_table(tw, k.tw_z, n);
     __syncthreads();
     const int f = blockIdx.z, x = blockIdx.y, y0 = blockIdx.x * P;
+    const int yv = min(P, k.ny - y0);  // rows of the tile inside the grid (even)
     const float* src = k.v[f];
     float2* Z = out_any<N, 8, kThreads, kLinePad>(k.pz, A, B);
     auto load = [&](int q, int i) -> float2 {
+        if (2 * q >= yv) return make_float2(0.f, 0.f);
         const int b = cell(k, x, y0 + 2 * q, i);
         return make_float2(src[b], src[b + n]);
     };
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
     float2* H = k.H[f];
     for (int t = threadIdx.x; t < k.nkz * P; t += blockDim.x) {
         const int p = t % P, kz = t / P, q = p >> 1;
+        if (p >= yv) continue;
         const float2 z = Z[q * ps + kz];
         const float2 zm = cconj(Z[q * ps + (kz ? n - kz : 0)]);
         H[spec(k, kz, x, y0 + p)] = (p & 1) ? unpack_b(z, zm) : unpack_a(z, zm);
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
 constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
 
 template <int N, bool INV>
-__global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long line0)
+__global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long line0, long long line_end)
 {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
@@ -141,13 +144,15 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     // forward: H -> Hy (H stays for k_sigma's kz-only fields); inverse: G in
     // place, blockIdx.y over the fields that went through k_mx
     const int c = blockIdx.y;
-    const long long off = (line0 + (long long)blockIdx.x * L) * n;
+    const long long first = line0 + (long long)blockIdx.x * L;
+    const int lv = (int)min((long long)L, line_end - first);  // lines of the tile inside the batch
+    const long long off = first * n;
     const float2* src = (INV ? k.G[c_gxy[c]] : k.H[c]) + off;
     float2* dst = (INV ? k.G[c_gxy[c]] : k.Hy[c]) + off;
     const bool ydv = !INV && k.Yv[c] != nullptr;
-    auto load = [&](int p, int i) -> float2 { return src[(long long)p * n + i]; };
+    auto load = [&](int p, int i) -> float2 { return p < lv ? src[(long long)p * n + i] : make_float2(0.f, 0.f); };
     auto store = [&](int p, int i, float2 v) {
-        dst[(long long)p * n + i] = v;
+        if (p < lv) dst[(long long)p * n + i] = v;
         if (ydv) C[p * n + i] = v;
     };
     fft_any<N, 8, kCyThreads, kLinePad, INV>(k.py, tw, A, B, L, n + n / 16, 1, load, store);
@@ -161,7 +166,9 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
             const float inv_n = 1.0f / ((float)n * (float)k.nz);
             float2* yd = k.Yv[c] + off;
             auto load_d = [&](int p, int i) -> float2 { return cmul(C[p * n + i], cscale(T[i], inv_n)); };
-            auto store_d = [&](int p, int i, float2 v) { yd[(long long)p * n + i] = v; };
+            auto store_d = [&](int p, int i, float2 v) {
+                if (p < lv) yd[(long long)p * n + i] = v;
+            };
             fft_any<N, 8, kCyThreads, kLinePad, true>(k.py, tw, A, B, L, n + n / 16, 1, load_d, store_d);
         }
     }
@@ -193,20 +200,22 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
     float* tkx = reinterpret_cast<float*>(tFBy + 2 * P);
     float* tky = tkx + n;                         // [P]
     const int kz = kz0 + blockIdx.y, y0 = blockIdx.x * P, c = blockIdx.z;
+    const int yv = min(P, k.ny - y0);  // rows of the tile inside the grid
     load_table(tw, k.tw_x, n);
     load_table(tFx, k.Fx, n);
     load_table(tBx, k.Bx, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) tkx[i] = k.kx[i];
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        tky[i] = k.ky[y0 + i];
-        tFBy[i] = k.Fy[y0 + i];
-        tFBy[P + i] = k.By[y0 + i];
+        const bool in = i < yv;
+        tky[i] = in ? k.ky[y0 + i] : 0.f;
+        tFBy[i] = in ? k.Fy[y0 + i] : make_float2(0.f, 0.f);
+        tFBy[P + i] = in ? k.By[y0 + i] : make_float2(0.f, 0.f);
     }
     __syncthreads();
 
     {
         const float2* H = k.Hy[c];
-        auto load = [&](int p, int i) -> float2 { return H[spec(k, kz, i, y0 + p)]; };
+        auto load = [&](int p, int i) -> float2 { return p < yv ? H[spec(k, kz, i, y0 + p)] : make_float2(0.f, 0.f); };
         auto store = [&](int p, int i, float2 v) { V[i * P + p] = v; };
         fft_any<N, 16, kThreads, kPencil, false>(k.px, tw, A, B, P, 1, P, load, store);
     }
@@ -235,7 +244,9 @@ __global__ void __launch_bounds__(kThreads) k_mx(KP k, int P_rt, int kz0)
                 else T = fw ? tFz : tBz;
                 return cmul(V[i * P + p], cscale(T, ap * k.inv_ntp));
             };
-            auto store = [&](int p, int i, float2 v) { G[spec(k, kz, i, y0 + p)] = v; };
+            auto store = [&](int p, int i, float2 v) {
+                if (p < yv) G[spec(k, kz, i, y0 + p)] = v;
+            };
             fft_any<N, 16, kThreads, kPencil, true>(k.px, tw, A, B, P, 1, P, load, store);
         }
     }
@@ -290,7 +301,10 @@ constexpr int sigma_cells(int n) { return (n == 256 && !sigma_inplace(n)) ? 2 : 
 // stress update; then the z derivatives of the new szz, sxz, syz for the next
 // velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
 // z terms, and the source injection.
-template <int N>
+//
+// RAG: the grid's last y tile is partial (ny not a multiple of the tile); a
+// separate instantiation, so the masks cost the full tiles no registers.
+template <int N, bool RAG>
 __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
 {
     constexpr bool INPLACE = sigma_inplace(N);
@@ -316,6 +330,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     float* ty = tz + 4 * n;                                               // [4][P]: ay by ayh byh of the rows
     float2* tzs = reinterpret_cast<float2*>(ty + 4 * P);                  // [2][n]: Fz Bz
     const int x = blockIdx.y, y0 = blockIdx.x * P;
+    const int yv = RAG ? min(P, ny - y0) : P;  // rows of the tile inside the grid (even)
     load_table(tw, k.tw_z, n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         tz[i] = k.az[i];
@@ -326,10 +341,11 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         tzs[n + i] = k.Bz[i];
     }
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
-        ty[i] = k.ay[y0 + i];
-        ty[P + i] = k.by[y0 + i];
-        ty[2 * P + i] = k.ayh[y0 + i];
-        ty[3 * P + i] = k.byh[y0 + i];
+        const bool in = !RAG || i < yv;
+        ty[i] = in ? k.ay[y0 + i] : 0.f;
+        ty[P + i] = in ? k.by[y0 + i] : 0.f;
+        ty[2 * P + i] = in ? k.ayh[y0 + i] : 0.f;
+        ty[3 * P + i] = in ? k.byh[y0 + i] : 0.f;
     }
     const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
     // where each of the 27 fields comes from: G (x/y passes), Yv (forward y
@@ -356,7 +372,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     auto prefetch_group = [&](int g) {
         if (g > 3) return;
         const int c0 = cell(k, x, y0, 0);
-        const unsigned run = 4u * P * n;
+        const unsigned run = 4u * yv * n;
         if (threadIdx.x == 0) {
             if (g == 0) {
                 const float* arr[13] = {k.s[0], k.s[1], k.s[2], k.Q[0], k.Q[1], k.Q[2], k.mrho, k.mgp, k.mgs,
@@ -385,6 +401,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         // round trip (normalised by 1/ntp) would have produced
         auto load = [&](int pp, int i) -> float2 {
             const int f = pp / Qp, q = pp - f * Qp, o = o0 + f;
+            if (RAG && 2 * q >= yv) return make_float2(0.f, 0.f);
             const int kk = i <= n / 2 ? i : n - i;
             const float4 gg = *reinterpret_cast<const float4*>(s_src[o] + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
@@ -409,12 +426,16 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             // as one float2, into the slot of the staging tile they came from:
             // every thread overwrites only its own inputs, no barrier or
             // register staging needed.  The update reads them through sval.
+            // Two-stage lengths take stage 1's twiddles in stage 0 (PRETW),
+            // which keeps the 256-point transform free of register spill;
+            // multi-round stages stay loops (ROLL) for the same reason at the
+            // lengths with small radices.
             if (grp == 0) {
-                using F = FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>;
+                using F = FftCT<N, 9 * kSigmaRows / 2, NT, kPencil, ct_nst(N) == 2, true>;
                 auto keep = [&](int pp, int i, float2 v) { Lb[F::at(pp, i)] = v; };
                 F::template run<true>(tw, A, B, load, keep);
             } else {
-                using F = FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>;
+                using F = FftCT<N, 6 * kSigmaRows / 2, NT, kPencil, ct_nst(N) == 2, true>;
                 auto keep = [&](int pp, int i, float2 v) { Lb[F::at(pp, i)] = v; };
                 F::template run<true>(tw, A, B, load, keep);
             }
@@ -454,7 +475,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
 #pragma unroll
                 for (int u = 0; u < kCells; ++u) {
                     const int t = t0 + u * blockDim.x;
-                    ok[u] = t < P * n;
+                    ok[u] = t < P * n && (!RAG || t / n < yv);
                     const int p = t / n, z = t - p * n;
                     ipv[u] = cell(k, x, y0 + p, z);
                     if (ok[u]) {
@@ -560,7 +581,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
 #pragma unroll
                 for (int u = 0; u < kCells; ++u) {
                     const int t = t0 + u * blockDim.x;
-                    ok[u] = t < P * n;
+                    ok[u] = t < P * n && (!RAG || t / n < yv);
                     const int p = t / n, z = t - p * n;
                     ipv[u] = cell(k, x, y0 + p, z);
                     if (ok[u]) {
@@ -628,7 +649,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         float2* B2 = (INPLACE && !two_buf) ? reinterpret_cast<float2*>(D) : B;
         float2* Zf = out_any<N, 3 * kSigmaRows / 2, NT, kLinePad>(k.pz, A, B2);
         auto store_f = [&](int pp, int i, float2 v) { Zf[pp * np1 + i] = v; };
-        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, false>(k.pz, tw, A, B2, npen, n + n / 16, 1, load, store_f);
+        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, false, true>(k.pz, tw, A, B2, npen, n + n / 16, 1, load, store_f);
         float2* X1 = Zf == A ? B2 : A;
         auto load_i = [&](int pp, int i) -> float2 {
             const int f = pp / Qp;
@@ -641,10 +662,11 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             D[(f * P + 2 * q) * np1 + i] = v.x;
             D[(f * P + 2 * q + 1) * np1 + i] = v.y;
         };
-        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i,
+        fft_any<N, 3 * kSigmaRows / 2, NT, kLinePad, true, true>(k.pz, tw, X1, Zf, npen, n + n / 16, 1, load_i,
                                                                  store_i);
         for (int t = threadIdx.x; t < 3 * P * n; t += blockDim.x) {
             const int i = t % n, fp = t / n, f = fp / P, p = fp - f * P;
+            if (RAG && p >= yv) continue;
             const int y = y0 + p;
             const int rc = f == 0 ? 2 : f == 1 ? 0 : 1;
             float* __restrict__ ph = k.php[f == 0 ? 8 : f == 1 ? 2 : 5];  // pzz_z, pxz_z, pyz_z
@@ -686,6 +708,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *k.d_it += 1;  // step counter
     __syncthreads();
     const int x = blockIdx.y, z0 = blockIdx.x * P;
+    const int zv = min(P, k.nz - z0);  // rows of the tile inside the grid (even)
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool xin = x < k.nx - 1;
     const float* __restrict__ sxy = k.s[3];
@@ -702,6 +725,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int p, int i) -> float2 {
+            if (p >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, x, i, z0 + p);
             return make_float2(sxy[ip], syy[ip]);
         };
@@ -727,9 +751,9 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
                 const int t = t0 + u * blockDim.x;
-                ok[u] = t < n * P;
                 pu[u] = t % P;
                 iu[u] = t / P;
+                ok[u] = t < n * P && pu[u] < zv;
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
@@ -763,6 +787,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int q, int i) -> float2 {
+            if (2 * q >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, x, i, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(syz + ip);
         };
@@ -783,9 +808,9 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
                 const int t = t0 + u * blockDim.x;
-                ok[u] = t < n * P;
                 pu[u] = t % P;
                 iu[u] = t / P;
+                ok[u] = t < n * P && pu[u] < zv;
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
@@ -828,6 +853,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     load_table(tF, k.Fx, n);
     __syncthreads();
     const int y = blockIdx.y, z0 = blockIdx.x * P;
+    const int zv = min(P, k.nz - z0);  // rows of the tile inside the grid (even)
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool yin = y < k.ny - 1;
     const float* __restrict__ sxx = k.s[0];
@@ -850,6 +876,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int p, int i) -> float2 {
+            if (p >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, i, y, z0 + p);
             return make_float2(sxx[ip], sxy[ip]);
         };
@@ -913,6 +940,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int q, int i) -> float2 {
+            if (2 * q >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, i, y, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
@@ -1235,6 +1263,39 @@ void dispatch_len(int n, F&& f)
 }
 constexpr int kCtLengths[] = {0, 64, 96, 100, 108, 120, 128, 144, 150, 160, 162, 180, 192, 200, 216, 240, 250, 256, 270, 288, 300, 320, 324, 360, 384, 512};
 
+namespace {
+
+bool ct_length(int n)
+{
+    for (int c : kCtLengths)
+        if (c > 0 && c == n) return true;
+    return false;
+}
+int cdiv(int a, int b) { return (a + b - 1) / b; }
+
+// Tiles of the step's launches.  A kernel whose transform length is compiled
+// takes its full tile along the other axis, the last tile ragged (its rows
+// or lines past the grid read as zeros and are not written); otherwise the
+// runtime path takes the largest power-of-two divisor of the tiled axis up
+// to the full tile.
+struct StepTiles {
+    int vy, vx, fz, cy, mx, sigma;
+};
+StepTiles step_tiles(const KP& k)
+{
+    auto tile = [](int len, int tiled, int want) { return ct_length(len) ? want : tile_of(tiled, want); };
+    StepTiles t;
+    t.vy = tile(k.ny, k.nz, 16);
+    t.vx = tile(k.nx, k.nz, 16);
+    t.fz = tile(k.nz, k.ny, 16);
+    t.cy = tile(k.ny, k.nx, 8);
+    t.mx = tile(k.nx, k.ny, 16);
+    t.sigma = tile(k.nz, k.ny, kSigmaRows);
+    return t;
+}
+
+}  // namespace
+
 int configure_kernels()
 {
     const int big = (int)kMaxSmem;  // leaves room for the kernels' small static tables
@@ -1250,7 +1311,8 @@ int configure_kernels()
             set((const void*)k_cy<N, false>);
             set((const void*)k_cy<N, true>);
             set((const void*)k_mx<N>);
-            set((const void*)k_sigma<N>);
+            set((const void*)k_sigma<N, false>);
+            if constexpr (N > 0) set((const void*)k_sigma<N, true>);
             set((const void*)k_vy<N>);
             set((const void*)k_vx<N>);
         });
@@ -1276,47 +1338,55 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     // the compile-time path of a kernel fixes its tile: 16 z rows (k_vy,
     // k_vx), 16 y rows (k_fz, k_mx), 8 lines (k_cy), kSigmaRows y rows
     auto len = [&](int n, int tile, int want) { return tile == want ? n : 0; };
+    const StepTiles T = step_tiles(k);
     mark(-1);
-    const int Pv = tile_of(k.nz, 16);
-    dispatch_len(len(k.ny, Pv, 16), [&](auto NN) {
-        k_vy<decltype(NN)::value><<<dim3(k.nz / Pv, k.nx), kThreads, smem_vyx(k.ny, Pv), st>>>(k, Pv);
+    dispatch_len(len(k.ny, T.vy, 16), [&](auto NN) {
+        k_vy<decltype(NN)::value><<<dim3(cdiv(k.nz, T.vy), k.nx), kThreads, smem_vyx(k.ny, T.vy), st>>>(k, T.vy);
     });
     mark(0);
-    dispatch_len(len(k.nx, Pv, 16), [&](auto NN) {
-        k_vx<decltype(NN)::value><<<dim3(k.nz / Pv, k.ny), kThreads, smem_vyx(k.nx, Pv), st>>>(k, Pv);
+    dispatch_len(len(k.nx, T.vx, 16), [&](auto NN) {
+        k_vx<decltype(NN)::value><<<dim3(cdiv(k.nz, T.vx), k.ny), kThreads, smem_vyx(k.nx, T.vx), st>>>(k, T.vx);
     });
     mark(1);
-    const int Pz = tile_of(k.ny, 16);
-    dispatch_len(len(k.nz, Pz, 16), [&](auto NN) {
-        k_fz<decltype(NN)::value><<<dim3(k.ny / Pz, k.nx, 3), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
+    dispatch_len(len(k.nz, T.fz, 16), [&](auto NN) {
+        k_fz<decltype(NN)::value><<<dim3(cdiv(k.ny, T.fz), k.nx, 3), kThreads, smem_fz(k, T.fz), st>>>(k, T.fz);
     });
     mark(2);
     // k-space passes, optionally in batches of kz planes (KP::kz_batch).
-    const int L = tile_of(k.nx, 8);
-    const int Pm = tile_of(k.ny, 16);
+    const int L = T.cy, Pm = T.mx;
     const int batch = k.kz_batch > 0 ? k.kz_batch : k.nkz;
     for (int kz0 = 0; kz0 < k.nkz; kz0 += batch) {
         const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
-        const long long line0 = (long long)kz0 * k.nx;
+        const long long line0 = (long long)kz0 * k.nx, line_end = line0 + (long long)nb * k.nx;
+        const int ncy = cdiv(nb * k.nx, L);
         dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, false><<<dim3(nb * k.nx / L, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L,
-                                                                                                             line0);
+            k_cy<decltype(NN)::value, false><<<dim3(ncy, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L, line0,
+                                                                                                  line_end);
         });
         mark(3);
         dispatch_len(len(k.nx, Pm, 16), [&](auto NN) {
-            k_mx<decltype(NN)::value><<<dim3(k.ny / Pm, nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
+            k_mx<decltype(NN)::value><<<dim3(cdiv(k.ny, Pm), nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
         });
         mark(4);
         dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, true><<<dim3(nb * k.nx / L, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L,
-                                                                                                           line0);
+            k_cy<decltype(NN)::value, true><<<dim3(ncy, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L, line0,
+                                                                                                 line_end);
         });
         mark(5);
     }
-    const int Ps = tile_of(k.ny, kSigmaRows);
+    const int Ps = T.sigma;
     dispatch_len(len(k.nz, Ps, kSigmaRows), [&](auto NN) {
         constexpr int N = decltype(NN)::value;
-        k_sigma<N><<<dim3(k.ny / Ps, k.nx), sigma_threads(N), smem_sigma(k, Ps, sigma_inplace(N)), st>>>(k, Ps);
+        const dim3 grid(cdiv(k.ny, Ps), k.nx);
+        const size_t sm = smem_sigma(k, Ps, sigma_inplace(N));
+        // the runtime path's tile divides ny; a compiled length may be ragged
+        if constexpr (N > 0) {
+            if (k.ny % Ps) {
+                k_sigma<N, true><<<grid, sigma_threads(N), sm, st>>>(k, Ps);
+                return;
+            }
+        }
+        k_sigma<N, false><<<grid, sigma_threads(N), sm, st>>>(k, Ps);
     });
     mark(6);
     if (k.rn > 0) {
@@ -1328,14 +1398,13 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
 // Largest dynamic shared memory of the step's launches for this grid.
 size_t step_smem_bytes(const KP& k)
 {
-    const int Pv = tile_of(k.nz, 16), Pz = tile_of(k.ny, 16), L = tile_of(k.nx, 8), Pm = tile_of(k.ny, 16);
-    const int Ps = tile_of(k.ny, kSigmaRows);
-    size_t m = smem_vyx(k.ny, Pv);
-    m = std::max(m, smem_vyx(k.nx, Pv));
-    m = std::max(m, smem_fz(k, Pz));
-    m = std::max(m, smem_cy(k, L, true));
-    m = std::max(m, smem_mx(k, Pm));
-    m = std::max(m, smem_sigma(k, Ps, false));  // the larger layout
+    const StepTiles T = step_tiles(k);
+    size_t m = smem_vyx(k.ny, T.vy);
+    m = std::max(m, smem_vyx(k.nx, T.vx));
+    m = std::max(m, smem_fz(k, T.fz));
+    m = std::max(m, smem_cy(k, T.cy, true));
+    m = std::max(m, smem_mx(k, T.mx));
+    m = std::max(m, smem_sigma(k, T.sigma, false));  // the larger layout
     return m;
 }
 
@@ -1364,11 +1433,11 @@ void launch_q_derivative(const KP& k_in, int axis, int fwd, int pw, float* out, 
     const int Pz = tile_of(k.ny, 16);
     k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);
     const int L = tile_of(k.nx, 8);
-    k_cy<0, false><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    k_cy<0, false><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0, (long long)k.nkz * k.nx);
     const int Pm = tile_of(k.ny, 8);
     kq_mx<<<dim3(k.ny / Pm, k.nkz), kThreads, sizeof(float2) * (k.nx + k.nx * Pm + 2 * (k.nx + k.nx / 16) * Pm), st>>>(
         k, Pm, axis, fwd, pw);
-    k_cy<0, true><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0);
+    k_cy<0, true><<<dim3(k.nkz * k.nx / L, 1), kCyThreads, smem_cy(k, L), st>>>(k, L, 0, (long long)k.nkz * k.nx);
     const int Pi = tile_of(k.ny, 8);
     kq_iz<<<dim3(k.ny / Pi, k.nx), kThreads, sizeof(float2) * (k.nz + 2 * (Pi / 2) * (k.nz + k.nz / 16)), st>>>(k, Pi,
                                                                                                                out);

@@ -97,15 +97,45 @@ def test_explosive_source_against_oracle(qvti, oracle):
 
 
 @pytest.mark.parametrize("n", [(64, 64, 64), (64, 128, 96), (160, 32, 48), (48, 144, 32), (32, 48, 192),
-                               (120, 32, 48), (32, 108, 48), (40, 48, 100)])
+                               (120, 32, 48), (32, 108, 48), (40, 48, 100),
+                               (64, 64, 100), (100, 108, 64), (64, 150, 64)])
 def test_compile_time_path_against_oracle(qvti, oracle, n):
     """A kernel takes the compile-time FFT path when its transform length is
-    compiled and its tile fits the grid; the mixed grids put some kernels on
-    it (x: k_vx, k_mx at 160 and 120; y: k_vy, k_cy at 144 and 108; z: k_fz,
-    k_sigma at the three-stage 192 and at 100) and the rest on the runtime
-    path.  VTI, heterogeneous,
-    receivers 6 cells above and within 3 cells of the source."""
+    compiled; the mixed grids put some kernels on it (x: k_vx, k_mx at 160
+    and 120; y: k_vy, k_cy at 144 and 108; z: k_fz, k_sigma at the
+    three-stage 192 and at 100) and the rest on the runtime path.  The last
+    three have partial last tiles: z tiles of k_vy and k_vx (nz = 100), y
+    tiles of k_fz and k_mx and the line tiles of k_cy (ny = 108, 33 x 100
+    lines), and the y tiles of k_sigma (ny = 150, the masked instantiation).
+    VTI, heterogeneous, receivers 6 cells above and within 3 cells of the
+    source."""
     nt = 100 if n[0] * n[1] * n[2] <= 64 ** 3 else 80
+    c = _ct_case(n, nt)
+    ours = qvti.run_case(c, snaps=[nt], vti=True)
+    ref = oracle.run_case(c, snaps=[nt], vti=True)
+    _compare(ours, ref, "ct%dx%dx%d" % n)
+
+
+@pytest.mark.parametrize("batch", [7, 17])
+def test_kz_batches_match_one_pass(qvti, batch):
+    """The k-space passes in batches of kz planes (ragged line tiles at every
+    batch edge: 7 x 100 and 17 x 100 lines are not multiples of 8) give the
+    same step bit for bit as one pass over all planes."""
+    n, nt = (100, 108, 64), 30
+    c = _ct_case(n, nt)
+    full = qvti.run_case(c, vti=True, want_state=True)
+    with qvti.simulation_for_case(c, vti=True) as sim:
+        qvti._check(qvti.lib().qvti_set_kz_batch(sim._h, batch), "qvti_set_kz_batch")
+        sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"], c["eps"], c["delta"])
+        sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])
+        sim.set_source(c["s_ix"], c["s_iy"], int(c["s_iz"]) + 10, np.asarray(c["rik"], np.float32)[:nt])
+        sim.reset()
+        sim.step(nt)
+        assert np.array_equal(sim.records(), full["rec"])
+        assert np.array_equal(sim.fields(0, 9), full["state"])
+
+
+def _ct_case(n, nt):
     c = qc.heterogeneous_case(n=n, pml=8, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=nt, f0=30.0, seed=21,
                               src=(n[0] // 2, n[1] // 2, n[2] // 2), r_iz=n[2] // 2 - 6, name="ct")
     # a 3 x 3 receiver patch beside the source: the direct wave reaches every
@@ -118,6 +148,4 @@ def test_compile_time_path_against_oracle(qvti, oracle, n):
     rng = np.random.default_rng(4)
     c["eps"] = (0.05 + 0.2 * rng.random(c["velp"].shape)).astype(np.float32)
     c["delta"] = (0.12 * rng.random(c["velp"].shape)).astype(np.float32)
-    ours = qvti.run_case(c, snaps=[nt], vti=True)
-    ref = oracle.run_case(c, snaps=[nt], vti=True)
-    _compare(ours, ref, "ct%dx%dx%d" % n)
+    return c
