@@ -23,10 +23,17 @@
 //                        (the reference's commented snapshot block,
 //                        cuviscoelas_3D.cu:1611-1627) to ./output/shot%dsnap%d_v?.bin
 //   outdir recdir        output directories (default ./output, ./record)
+//   log                  JSON-lines run log, one line per shot (default
+//                        <outdir>/run.jsonl; "none" disables): shot index,
+//                        wall seconds, Gcell-steps/s, status and, for
+//                        stepped runs (snap_every > 0), the FP64 sums of
+//                        squares of the nine wavefields after the last step
+//                        and whether any value was non-finite
 //
 // Outputs (formats of viscoelas_3D.cpp:188-199, 416-435):
 //   <outdir>/source_xy.txt, <outdir>/source_trnum.txt       text
 //   <recdir>/Q1dep_v{x,y,z}_small_shot%d.bin                raw float32 [it][ir]
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -109,6 +116,7 @@ int main(int argc, char** argv)
     const float w0 = (float)(2 * 3.1415926 * f0);  // viscoelas_3D.cpp:109
     const int snap_every = (int)p.num("snap_every", 0);
     const std::string outdir = p.str("outdir", "./output"), recdir = p.str("recdir", "./record");
+    const std::string log_path = p.str("log", (outdir + "/run.jsonl").c_str());
     const int ntx = nx + 2 * pml, nty = ny + 2 * pml, ntz = nz + 2 * pml;  // viscoelas_3D.cpp:117-119
     const int ntp = ntx * nty * ntz;
     mkdir(outdir.c_str(), 0755);
@@ -182,8 +190,14 @@ int main(int argc, char** argv)
     cuda_Device_malloc(ntx, nty, ntz, ntp, nx, ny, nz, nt, rnmax, plan.data(), GPU_N);
     cuda_Host_initialization(ntp, nt, rnmax, plan.data(), GPU_N);
 
+    FILE* log = log_path == "none" ? nullptr : std::fopen(log_path.c_str(), "w");
+    if (!log && log_path != "none") std::fprintf(stderr, "cannot write %s\n", log_path.c_str());
     int status = 0;
     for (int is = 0; is < ns; is += GPU_N) {
+        const auto t0 = std::chrono::steady_clock::now();
+        int shot_rc = 0;
+        double norms[9];
+        int nonfinite = -1;  // -1: not measured (a whole-shot ABI call)
         if (snap_every > 0) {
             // stepped run through the extended ABI to take snapshots
             qvti_config cfg{};
@@ -214,19 +228,37 @@ int main(int argc, char** argv)
                 }
             }
             if (!rc) rc = qvti_get_records(sim, plan[0].record, plan[0].record2, plan[0].record3);
+            if (!rc) {
+                const int nrc = qvti_field_norms(sim, norms, &nonfinite);
+                if (nrc && nrc != QVTI_ERR_NONFINITE) rc = nrc;
+            }
             if (sim) qvti_destroy(sim);
             if (rc) {
                 std::fprintf(stderr, "shot %d failed: %s\n", is, qvti_error_string(rc));
                 status = 1;
             }
+            shot_rc = rc;
         } else {
             cuda_forward_acoustic_3D(0, is, nt, ntx, nty, ntz, ntp, nx, ny, nz, pml, dx, dy, dz, dt, f0, w0, 5000.0f,
                                      rik.data(), velp.data(), gama_p.data(), vels.data(), gama_s.data(), rho.data(),
                                      ss.data(), plan.data(), GPU_N, rnmax, rnx_max, rny_max, dr);
-            if (qvti_last_error()) {
-                std::fprintf(stderr, "shot %d failed: %s\n", is, qvti_error_string(qvti_last_error()));
+            shot_rc = qvti_last_error();
+            if (shot_rc) {
+                std::fprintf(stderr, "shot %d failed: %s\n", is, qvti_error_string(shot_rc));
                 status = 1;
             }
+        }
+        const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (log) {
+            std::fprintf(log, "{\"shot\": %d, \"seconds\": %.6f, \"gcell_steps_per_s\": %.6f, \"status\": \"%s\"", is,
+                         sec, (double)ntp * nt / sec / 1e9, shot_rc ? qvti_error_string(shot_rc) : "ok");
+            if (nonfinite >= 0) {
+                std::fprintf(log, ", \"nonfinite\": %s, \"energy\": [", nonfinite ? "true" : "false");
+                for (int f = 0; f < 9; ++f) std::fprintf(log, "%s%.17g", f ? ", " : "", norms[f]);
+                std::fprintf(log, "]");
+            }
+            std::fprintf(log, "}\n");
+            std::fflush(log);
         }
         for (int i = 0; i < GPU_N && is + i < ns; i++) {
             const char* comp[3] = {"vx", "vy", "vz"};
@@ -240,5 +272,6 @@ int main(int argc, char** argv)
         std::printf("shot %d done\n", is);
     }
     cuda_Device_free(plan.data(), GPU_N);
+    if (log) std::fclose(log);
     return status;
 }

@@ -6,8 +6,10 @@ per shot and component) on top of the drop-in C ABI.
 A two-shot run on a 32^3 padded grid: the files the reference writes exist
 with their sizes and formats, and each shot's seismograms equal the same
 shot run through the Python binding of the extended ABI (bit for bit: same
-kernels, same inputs).
+kernels, same inputs).  The JSON-lines run log has one line per shot; a
+stepped run adds the energy norms, which equal the binding's.
 """
+import json
 import os
 import subprocess
 
@@ -71,6 +73,10 @@ def test_driver_writes_the_reference_outputs(qvti, tmp_path):
             assert a.size == desc["nt"] * rn
             assert np.array_equal(a.reshape(desc["nt"], rn), ref[i])
         assert np.abs(ref[0]).max() > 0
+    log = [json.loads(line) for line in (out / "run.jsonl").read_text().splitlines()]
+    assert [e["shot"] for e in log] == [0, 1]
+    assert all(e["status"] == "ok" and e["seconds"] > 0 and e["gcell_steps_per_s"] > 0 for e in log)
+    assert all("energy" not in e for e in log)  # whole-shot ABI calls: no wavefield access
 
 
 def test_driver_snapshots_match_fields(qvti, tmp_path):
@@ -84,3 +90,8 @@ def test_driver_snapshots_match_fields(qvti, tmp_path):
             want = res["snaps"][k][i][pml:-pml, pml:-pml, pml:-pml]
             assert a.size == want.size
             assert np.array_equal(a.reshape(want.shape), want)
+    (entry,) = [json.loads(line) for line in (out / "run.jsonl").read_text().splitlines()]
+    assert entry["shot"] == 0 and entry["status"] == "ok" and entry["nonfinite"] is False
+    state = qvti.run_case(c, want_state=True)["state"].astype(np.float64)
+    want = (state.reshape(9, -1) ** 2).sum(axis=1)
+    assert np.allclose(entry["energy"], want, rtol=1e-9, atol=0)
