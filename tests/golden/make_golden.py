@@ -119,7 +119,7 @@ def save_case(outdir, c, snaps, lib=None):
 
 
 def main():
-    outdir = sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/golden"
+    outdir = sys.argv[1] if len(sys.argv) > 1 else "golden_out"
     os.makedirs(outdir, exist_ok=True)
     for c, snaps in golden_cases():
         save_case(outdir, c, snaps)
