@@ -692,7 +692,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
 // and P consecutive z; C-PML y terms; accumulate into R.  Each pass parks its
 // derivatives in shared memory; the epilogue then loads everything a cell
 // needs before storing anything (no store can delay a later load).
-template <int N>
+template <int N, bool RAG>
 __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 {
     const int P = N > 0 ? 16 : P_rt;
@@ -708,7 +708,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *k.d_it += 1;  // step counter
     __syncthreads();
     const int x = blockIdx.y, z0 = blockIdx.x * P;
-    const int zv = min(P, k.nz - z0);  // rows of the tile inside the grid (even)
+    const int zv = RAG ? min(P, k.nz - z0) : P;  // rows of the tile inside the grid (even)
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool xin = x < k.nx - 1;
     const float* __restrict__ sxy = k.s[3];
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int p, int i) -> float2 {
-            if (p >= zv) return make_float2(0.f, 0.f);
+            if (RAG && p >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, x, i, z0 + p);
             return make_float2(sxy[ip], syy[ip]);
         };
@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                 const int t = t0 + u * blockDim.x;
                 pu[u] = t % P;
                 iu[u] = t / P;
-                ok[u] = t < n * P && pu[u] < zv;
+                ok[u] = t < n * P && (!RAG || pu[u] < zv);
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
@@ -787,7 +787,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.py, A, B);
         auto load = [&](int q, int i) -> float2 {
-            if (2 * q >= zv) return make_float2(0.f, 0.f);
+            if (RAG && 2 * q >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, x, i, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(syz + ip);
         };
@@ -810,7 +810,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                 const int t = t0 + u * blockDim.x;
                 pu[u] = t % P;
                 iu[u] = t / P;
-                ok[u] = t < n * P && pu[u] < zv;
+                ok[u] = t < n * P && (!RAG || pu[u] < zv);
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
@@ -838,7 +838,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
 // x-derivatives of sxx (-, vx), sxy (+, vy), sxz (+, vz); C-PML x terms and
 // the velocity update (cuda_kernel_calculate_v, cu:1018-1101); same
 // park-then-epilogue structure as k_vy.
-template <int N>
+template <int N, bool RAG>
 __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
 {
     const int P = N > 0 ? 16 : P_rt;
@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     load_table(tF, k.Fx, n);
     __syncthreads();
     const int y = blockIdx.y, z0 = blockIdx.x * P;
-    const int zv = min(P, k.nz - z0);  // rows of the tile inside the grid (even)
+    const int zv = RAG ? min(P, k.nz - z0) : P;  // rows of the tile inside the grid (even)
     const float dt = k.dt, inv_n = 1.0f / n;
     const bool yin = y < k.ny - 1;
     const float* __restrict__ sxx = k.s[0];
@@ -876,7 +876,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
     {
         float2* Zf = out_any<N, 16, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int p, int i) -> float2 {
-            if (p >= zv) return make_float2(0.f, 0.f);
+            if (RAG && p >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, i, y, z0 + p);
             return make_float2(sxx[ip], sxy[ip]);
         };
@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         const int Qp = P / 2;
         float2* Zf = out_any<N, 8, kThreads, kPencil>(k.px, A, B);
         auto load = [&](int q, int i) -> float2 {
-            if (2 * q >= zv) return make_float2(0.f, 0.f);
+            if (RAG && 2 * q >= zv) return make_float2(0.f, 0.f);
             const int ip = cell(k, i, y, z0 + 2 * q);
             return *reinterpret_cast<const float2*>(sxz + ip);
         };
@@ -1313,8 +1313,12 @@ int configure_kernels()
             set((const void*)k_mx<N>);
             set((const void*)k_sigma<N, false>);
             if constexpr (N > 0) set((const void*)k_sigma<N, true>);
-            set((const void*)k_vy<N>);
-            set((const void*)k_vx<N>);
+            set((const void*)k_vy<N, false>);
+            set((const void*)k_vx<N, false>);
+            if constexpr (N > 0) {
+                set((const void*)k_vy<N, true>);
+                set((const void*)k_vx<N, true>);
+            }
         });
     set((const void*)k_deriv1d);
     set((const void*)kq_mx);
@@ -1340,12 +1344,32 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     auto len = [&](int n, int tile, int want) { return tile == want ? n : 0; };
     const StepTiles T = step_tiles(k);
     mark(-1);
+    // the runtime path's tiles divide the grid; a compiled length may be
+    // ragged (a separate instantiation carries the masks)
     dispatch_len(len(k.ny, T.vy, 16), [&](auto NN) {
-        k_vy<decltype(NN)::value><<<dim3(cdiv(k.nz, T.vy), k.nx), kThreads, smem_vyx(k.ny, T.vy), st>>>(k, T.vy);
+        constexpr int N = decltype(NN)::value;
+        const dim3 grid(cdiv(k.nz, T.vy), k.nx);
+        const size_t sm = smem_vyx(k.ny, T.vy);
+        if constexpr (N > 0) {
+            if (k.nz % T.vy) {
+                k_vy<N, true><<<grid, kThreads, sm, st>>>(k, T.vy);
+                return;
+            }
+        }
+        k_vy<N, false><<<grid, kThreads, sm, st>>>(k, T.vy);
     });
     mark(0);
     dispatch_len(len(k.nx, T.vx, 16), [&](auto NN) {
-        k_vx<decltype(NN)::value><<<dim3(cdiv(k.nz, T.vx), k.ny), kThreads, smem_vyx(k.nx, T.vx), st>>>(k, T.vx);
+        constexpr int N = decltype(NN)::value;
+        const dim3 grid(cdiv(k.nz, T.vx), k.ny);
+        const size_t sm = smem_vyx(k.nx, T.vx);
+        if constexpr (N > 0) {
+            if (k.nz % T.vx) {
+                k_vx<N, true><<<grid, kThreads, sm, st>>>(k, T.vx);
+                return;
+            }
+        }
+        k_vx<N, false><<<grid, kThreads, sm, st>>>(k, T.vx);
     });
     mark(1);
     dispatch_len(len(k.nz, T.fz, 16), [&](auto NN) {
