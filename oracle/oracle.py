@@ -65,6 +65,8 @@ def _full(c, key, shape):
     a = np.asarray(c[key], np.float32)
     if a.ndim == 0:
         a = np.full(shape, a, np.float32)
+    if a.shape != shape:  # the C restatement indexes the full grid
+        raise ValueError("%s has shape %s, the grid is %s" % (key, a.shape, shape))
     return np.ascontiguousarray(a)
 
 
