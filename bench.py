@@ -18,8 +18,11 @@ one JSON line each for those forms; the default is the 256^3 step.
 ``--impl reference`` times the reference's CPU counterpart: the reference has
 no CPU implementation of the path (it is CUDA + cuFFT), so the arm runs the
 FP64 CPU restatement (oracle/) on all host cores, each step a bounded sample
-(one time step of a centred crop of the same model, crop sized so the whole
-run ends in a few minutes), on rank 0 only.
+(one time step of the centred 128^3 crop of the same model, at most 20 timed
+steps so the run ends in a few minutes), on rank 0 only.  Our arm's
+``cpu_baseline`` times the same crop the same way with 4 steps, and its
+``reference_gpu`` entry times the reference's own cuFFT build on this GPU
+(256^3 isotropic, outside the timed region).
 """
 import argparse
 import contextlib
@@ -203,34 +206,54 @@ def workload_desc(dt):
 
 
 # ----------------------------------------------------------------- CPU leg --
-def oracle_rate(model, crop, steps, warmup, dt, nthreads):
-    """Gcell-steps/s of the FP64 oracle on a centred crop^3 of the model (the
-    crop no larger than the grid).  Returns (rate, seconds, crop)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as orc
+CPU_CROP = 128  # edge of the centred crop both CPU legs time (clamped to the grid)
+
+
+def oracle_case(model, crop, nt, dt):
+    """Case dict of a centred crop^3 of the model (crop clamped to the grid)."""
     crop = min(crop, min(GRID))
     c0 = [(g - crop) // 2 for g in GRID]
     sl = tuple(slice(a, a + crop) for a in c0)
     pml = max(4, min(PML, crop // 6))
-    case = dict(ntx=crop, nty=crop, ntz=crop, pml=pml, nt=steps + warmup, dx=DX, dy=DX, dz=DX, dt=dt, f0=F0,
+    case = dict(ntx=crop, nty=crop, ntz=crop, pml=pml, nt=nt, dx=DX, dy=DX, dz=DX, dt=dt, f0=F0,
                 s_ix=crop // 2, s_iy=crop // 2, s_iz=pml + 5, r_iz=pml, r_ix=np.arange(crop, dtype=np.int32),
                 r_iy=np.full(crop, crop // 2, np.int32), rnx_max=crop, rny_max=1)
     for k in ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta"):
         case[k] = np.ascontiguousarray(model[k][sl])
     models = _load("qvti_models", os.path.join(PKG, "models.py"))
-    case["rik"] = models.ricker(steps + warmup, dt, F0)
+    case["rik"] = models.ricker(nt, dt, F0)
+    return case, crop
+
+
+def oracle_rate(model, crop, steps, dt, nthreads):
+    """Gcell-steps/s of the FP64 oracle on a centred crop^3 of the model.
+
+    Two runs of the same case, of 1 and 1 + `steps` steps: their difference
+    is the time of `steps` steps with the setup (tables, coefficients) and
+    the first step cancelled; the 1-step run is the warm-up.  At the default
+    128^3 crop a step takes seconds, far above timing noise.  Returns (rate,
+    seconds of the timed steps, crop)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    case, crop = oracle_case(model, crop, 1 + steps, dt)
     t0 = time.perf_counter()
-    orc.run_case(case, nt=max(warmup, 1), vti=True, ref_offset=False, nthreads=nthreads)
+    orc.run_case(case, nt=1, vti=True, ref_offset=False, nthreads=nthreads)
     t1 = time.perf_counter()
-    orc.run_case(case, nt=max(warmup, 1) + steps, vti=True, ref_offset=False, nthreads=nthreads)
+    orc.run_case(case, nt=1 + steps, vti=True, ref_offset=False, nthreads=nthreads)
     t2 = time.perf_counter()
-    sec = (t2 - t1) - (t1 - t0)  # the extra `steps` steps, setup cancelled
-    if sec < 0.1 * (t2 - t1):
-        # the difference is within timing noise (few steps of a small crop):
-        # the longer run's own time, setup included, bounds the rate below
-        sec = t2 - t1
-        return crop ** 3 * (max(warmup, 1) + steps) / sec / 1e9, sec * steps / (max(warmup, 1) + steps), crop
+    sec = (t2 - t1) - (t1 - t0)
+    if sec <= 0:
+        raise RuntimeError("oracle timing: %d steps took no measurable time (%.3f s, %.3f s)"
+                           % (steps, t1 - t0, t2 - t1))
     return crop ** 3 * steps / sec / 1e9, sec, crop
+
+
+def cpu_sample(crop, steps, sec, cores):
+    return ("FP64 CPU restatement (oracle/) on a centred %d^3 crop of the same model: %d timed steps (%.1f s), "
+            "setup and first step cancelled by differencing a 1-step and a %d-step run, %d threads; the rate "
+            "per cell-step is taken as the %dx%dx%d rate (not scaled for the FFTs' log n growth, %.2fx at "
+            "that size)" % (crop, steps, sec, 1 + steps, cores, GRID[0], GRID[1], GRID[2],
+                             math.log(GRID[0] * GRID[1] * GRID[2]) / math.log(crop ** 3)))
 
 
 def reference_arm(args, world, rank):
@@ -239,27 +262,89 @@ def reference_arm(args, world, rank):
     models = _load("qvti_models", os.path.join(PKG, "models.py"))
     model, dt, _, _ = make_model(models)
     cores = os.cpu_count() or 1
-    # size the crop so that warmup + steps oracle steps take ~150 s
-    probe_rate, _, _ = oracle_rate(model, 32, 2, 1, dt, cores)
-    budget = 150.0 / max(args.steps + args.warmup, 1)
-    crop = int((probe_rate * 1e9 * budget) ** (1 / 3) * 0.7)
-    crop = max(32, min(192, crop // 16 * 16))
-    rate, sec, crop = oracle_rate(model, crop, args.steps, args.warmup, dt, cores)
+    # each timed step is one step of the crop (a bounded sample of the
+    # workload's step); at most 20 of them so the arm ends in a few minutes
+    steps = max(1, min(args.steps, 20))
+    rate, sec, crop = oracle_rate(model, CPU_CROP, steps, dt, cores)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": workload_desc(dt), "sample": "%d^3 crop" % crop},
+        "data": "synthetic", "config": {"workload": workload_desc(dt), "sample": "%d^3 crop" % crop,
+                                        "timed_steps": steps},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": "FP64 CPU restatement (oracle/), %d timed steps of a centred %d^3 crop of the "
-                                   "same model, %d threads" % (args.steps, crop, cores)},
+                         "sample": cpu_sample(crop, steps, sec, cores)},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def reference_gpu_timing(n, pml):
+    """The reference's own cuFFT build (oracle/_ref, compiled from its
+    unmodified sources) timed on the same B200 by oracle/time_reference.py in
+    a separate process, outside this bench's timed region: 256^3 isotropic
+    (the reference has no VTI), per-step time from the difference of a 45-
+    and a 25-step call, beside this library's isotropic and VTI steps on the
+    same case.  None when the build is absent."""
+    so = os.path.join(ROOT, "oracle", "_ref", "libqvti_ref.so")
+    if not os.path.exists(so):
+        return None
+    try:
+        out = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "time_reference.py"), str(n), str(pml)],
+                             capture_output=True, text=True, timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"error": "timed out"}
+    res = {}
+    for line in out.stdout.splitlines():
+        p = line.split()
+        if len(p) == 4 and p[1] == "n=%d" % n:
+            res[p[0]] = {"ms_per_step": float(p[2].split("=")[1]), "gcell_steps_per_s": float(p[3].split("=")[1])}
+    if "reference_cufft" not in res:
+        return {"error": (out.stderr or out.stdout)[-300:]}
+    r = res["reference_cufft"]["ms_per_step"]
+    return {"grid": [n, n, n], "pml": pml, "medium": "isotropic homogeneous", "timing": res,
+            "speedup_iso": r / res["library_iso"]["ms_per_step"] if "library_iso" in res else None,
+            "source": "oracle/_ref (reference cuviscoelas_3D.cu + cuFFT, unmodified, sm_100a), wall time of "
+                      "cuda_forward_acoustic_3D: (t(45) - t(25)) / 20"}
+
+
 # ----------------------------------------------------------------- our arm --
+def tc_form(qv, sim, K, W, nprof, ntp, world, dist, ms_plain):
+    """The split-precision tensor-core form on the same simulation: W warm-up
+    and K timed steps (CUDA events on the engine's stream, max over ranks),
+    its per-kernel times, and its agreement with the plain form: both forms
+    run the same 60 steps from rest and their seismograms and final
+    velocities are compared (relative L2)."""
+    try:
+        sim.set_form(qv.FORM_TC)
+    except qv.QvtiError as e:
+        return {"unavailable": str(e)}
+    sim.step(W)
+    sim.sync()
+    dist.barrier()
+    ms = dist.max(sim.step_timed(K))
+    kernels = sim.profile_step(nprof)
+    value = aggregate_value(ntp, K, world, ms)
+    agree = {}
+    runs = {}
+    for form in (qv.FORM_PLAIN, qv.FORM_TC):
+        sim.set_form(form)
+        sim.reset()
+        sim.step(60)
+        runs[form] = (sim.records(), sim.fields(0, 3))
+    sim.set_form(qv.FORM_TC)
+    rel = lambda a, b: float(np.linalg.norm((a - b).astype(np.float64)) / max(np.linalg.norm(b.astype(np.float64)), 1e-30))
+    for i, comp in enumerate(("vx", "vy", "vz")):
+        agree["rec_" + comp] = rel(runs[qv.FORM_TC][0][i], runs[qv.FORM_PLAIN][0][i])
+        agree["field_" + comp] = rel(runs[qv.FORM_TC][1][i], runs[qv.FORM_PLAIN][1][i])
+    return {"form": "256-point y transforms as 16-point DFT products on tcgen05 (kind::tf32, 3 hi/lo terms, FP32 "
+                    "accumulate in TMEM); other transforms FP32",
+            "value": value, "ms_per_step": ms / K, "tc_vs_plain": (ms_plain / K) / (ms / K),
+            "kernels": [{"name": n, "ms": round(m, 4), "gbs": round(b / (m / 1e3) / 1e9, 1)} for n, m, b in kernels],
+            "relL2_vs_plain_60_steps": agree}
+
+
 def our_arm(args, world, rank, local):
     qv = _load("qvti_b200", os.path.join(PKG, "qvti.py"))
     models = _load("qvti_models", os.path.join(PKG, "models.py"))
@@ -269,7 +354,7 @@ def our_arm(args, world, rank, local):
     ntp = nx * ny * nz
     K, W = args.steps, args.warmup
     nprof = 3
-    nt = W + K + nprof
+    nt = 2 * (W + K + nprof) + 60  # the plain form, the tensor-core form, their 60-step comparison
     rik = models.ricker(nt, dt, F0)
     r_ix, r_iy = models.surface_receivers(nx, ny)
     src = (nx // 2, ny // 2, PML + 5)
@@ -293,6 +378,7 @@ def our_arm(args, world, rank, local):
 
     kernels = sim.profile_step(nprof)
     norms, nonfinite, _ = sim.norms()
+    tc = None if args.no_tc else tc_form(qv, sim, K, W, nprof, ntp, world, dist, ms_max)
     sim.close()
 
     if args.no_e2e:
@@ -340,11 +426,14 @@ def our_arm(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        # the reference arm's crop and method, fewer timed steps (about 20 s
+        # of CPU work)
         cores = os.cpu_count() or 1
-        rate, sec, crop = oracle_rate(model, 96, 6, 1, dt, cores)
-        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": "FP64 CPU restatement (oracle/) on a centred %d^3 crop of the same model, 6 timed "
-                         "steps (%.1f s), %d threads" % (crop, sec, cores)}
+        rate, sec, crop = oracle_rate(model, CPU_CROP, 4, dt, cores)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": cpu_sample(crop, 4, sec, cores)}
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_timing(GRID[0], PML)
 
     if rank == 0:
         line = {
@@ -362,6 +451,8 @@ def our_arm(args, world, rank, local):
                               "canonical_B_alg_T63": 1177},
             "kernels": [{"name": n, "ms": round(m, 4), "gbs": round(b / (m / 1e3) / 1e9, 1)} for n, m, b in kernels],
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
+            "tc": tc,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                     "seconds": t_e2e},
             "gpu_launches": len(kernels) * K,
@@ -514,6 +605,88 @@ def serve_arm(args):
     return 0
 
 
+# ------------------------------------------------------ precision form --
+def precision_arm(args):
+    """Precision form: the VTI generator at 512 x 512 x 256 (seed 2024, its
+    own perturbation fields, dt from its stability bound), pml 30, 20 Hz
+    force at (256, 256, 35), receivers every 4th surface point; --nt steps
+    (3000) from rest in the plain FP32 form and, where the grid has one, the
+    tensor-core form, each timed whole with CUDA events.  Accuracy: the
+    centred 128^3 crop of the same model (400 steps) run in each form and
+    compared with the FP64 oracle's run of that crop
+    (tests/golden/oracle/vti512_crop128.npz): relative L2 of each seismogram
+    component and of vx, vy, vz on two planes every 100 steps (worst over
+    the snapshots), and the peak seismogram error max|d| / max|ref|."""
+    qv = _load("qvti_b200", os.path.join(PKG, "qvti.py"))
+    md = _load("qvti_models", os.path.join(PKG, "models.py"))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import make_oracle_golden as mog
+    shape, pml, nt = (512, 512, 256), 30, args.nt
+    model = md.layered_vti(shape, DX, seed=SEED)
+    dt, lim, _ = md.choose_dt(model, DX, F0, DT_NOMINAL, vti=True)
+    gx = np.arange(0, shape[0], 4, dtype=np.int32)
+    gy = np.arange(0, shape[1], 4, dtype=np.int32)
+    r_ix, r_iy = np.repeat(gx, gy.size), np.tile(gy, gx.size)
+    rik = md.ricker(nt, dt, F0)
+    forms = {}
+    with qv.Simulation(*shape, pml, DX, DX, DX, dt, F0, vti=True) as sim:
+        sim.set_model(*[model[k] for k in ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta")])
+        sim.set_receivers(pml, r_ix, r_iy)
+        sim.set_source(shape[0] // 2, shape[1] // 2, pml + 5, rik)
+        for name, form in (("plain", qv.FORM_PLAIN), ("tc", qv.FORM_TC)):
+            try:
+                sim.set_form(form)
+            except qv.QvtiError as e:
+                forms[name] = {"unavailable": str(e)}
+                continue
+            sim.reset()
+            sim.step(5)  # graph build and first launches, untimed
+            sim.reset()
+            with ClockSampler(0) as clk:
+                ms = sim.step_timed(nt)
+            norms, bad, _ = sim.norms()
+            forms[name] = {"value": shape[0] * shape[1] * shape[2] * nt / (ms / 1e3) / 1e9, "seconds": ms / 1e3,
+                           "ms_per_step": ms / nt, "finite": not bad, "clocks": clk.summary()}
+    crop = mog.crop128_case(shape, "vti512_crop128", 400, model=model)
+    del model
+    path = os.path.join(ROOT, "tests", "golden", "oracle", "vti512_crop128.npz")
+    acc = {}
+    if os.path.exists(path):
+        g = dict(np.load(path))
+        snaps = list(range(100, 401, 100))
+        for name, form in (("plain", qv.FORM_PLAIN), ("tc", qv.FORM_TC)):
+            try:
+                ours = qv.run_case(crop, snaps=snaps, vti=True, ref_offset=False, form=form)
+            except qv.QvtiError as e:
+                acc[name] = {"unavailable": str(e)}
+                continue
+            rel = lambda a, b: float(np.linalg.norm((a - b).astype(np.float64)) / np.linalg.norm(b.astype(np.float64)))
+            e = {}
+            for i, comp in enumerate(("vx", "vy", "vz")):
+                e["rec_" + comp] = rel(ours["rec"][i], g["rec_" + comp])
+                e["field_" + comp] = max(max(rel(ours["snaps"][k][i][:, int(crop["plane_y"]), :], g["plane_y_%d" % k][i]),
+                                             rel(ours["snaps"][k][i][:, :, int(crop["plane_z"])], g["plane_z_%d" % k][i]))
+                                         for k in snaps)
+            ref = np.stack([g["rec_vx"], g["rec_vy"], g["rec_vz"]])
+            e["peak_seismogram_err"] = float(np.abs(ours["rec"] - ref).max() / np.abs(ref).max())
+            e["worst_relL2"] = max(v for k, v in e.items() if k != "peak_seismogram_err")
+            acc[name] = e
+    else:
+        acc = {"unavailable": "oracle fixture tests/golden/oracle/vti512_crop128.npz missing"}
+    out = {"metric": "Gcell-steps/s 512x512x256 VTI, %d steps; per-field relL2 vs FP64 oracle (128^3 crop)" % nt,
+           "value": forms["plain"]["value"], "unit": UNIT, "higher_is_better": True, "n_gpus": 1, "dtype": "f32",
+           "data": "synthetic", "forms": forms, "accuracy_crop128_400_steps": acc,
+           "config": {"workload": "precision form: VTI generator at 512x512x256 (6 layers, eps/delta/Q per layer, 5%% "
+                                  "Gaussian perturbations, seed %d), pml %d, dt %.2f ms (0.8 ms capped to 80%% of the "
+                                  "stability bound %.2f ms), 20 Hz force at (256,256,%d), receivers every 4th surface "
+                                  "point; accuracy on the centred 128^3 crop (pml 20, 400 steps) against the FP64 "
+                                  "oracle" % (SEED, pml, dt * 1e3, lim * 1e3, pml + 5),
+                      "grid": list(shape), "steps": nt}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -522,8 +695,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's cuFFT build")
+    ap.add_argument("--no-tc", action="store_true", help="skip the tensor-core form")
     ap.add_argument("--grid", type=int, default=256, help="cube edge (profiling of smaller cases)")
-    ap.add_argument("--workload", default="step", choices=["step", "batch", "serve"])
+    ap.add_argument("--workload", default="step", choices=["step", "batch", "serve", "precision"])
+    ap.add_argument("--nt", type=int, default=3000, help="precision: steps of the 512x512x256 run")
     ap.add_argument("--shots", type=int, default=48, help="batch: number of shots")
     ap.add_argument("--nt-scale", type=float, default=0.1, help="batch/serve: fraction of the nominal nt")
     ap.add_argument("--rate", type=float, default=4.0, help="serve: arrivals per second")
@@ -533,6 +709,8 @@ def main():
         return batch_arm(args)
     if args.workload == "serve":
         return serve_arm(args)
+    if args.workload == "precision":
+        return precision_arm(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = dist_setup()

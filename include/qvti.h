@@ -49,9 +49,11 @@ typedef struct {
                            reference's pi (viscoelas_3D.cpp:109)                              */
 } qvti_config;
 
-/* Device memory the engine needs for a grid (bytes).  Replaces the sizing
- * implicit in cuda_Device_malloc (cuviscoelas_3D.cu:1689-1916). */
-size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int vti);
+/* Device memory the engine needs for a grid with `pml` C-PML cells per face
+ * (bytes; the C-PML memory variables are stored for their slabs only).
+ * Replaces the sizing implicit in cuda_Device_malloc
+ * (cuviscoelas_3D.cu:1689-1916). */
+size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int pml, int vti);
 
 /* Allocate a simulation on cfg->device.  Replaces cuda_Device_malloc
  * (Myfunctions.h:91-96, cuviscoelas_3D.cu:1689-1916). */
@@ -60,6 +62,17 @@ int qvti_create(const qvti_config* cfg, qvti_sim** out);
 /* Free everything.  Replaces cuda_Device_free (Myfunctions.h:98-102,
  * cuviscoelas_3D.cu:1922-2141). */
 int qvti_destroy(qvti_sim* sim);
+
+/* The configuration a simulation was created with.  Lets a caller reuse a
+ * simulation for the next shot when grid, spacing, dt and frequency are
+ * unchanged, as the reference reuses the buffers of cuda_Device_malloc across
+ * its shot loop (viscoelas_3D.cpp:355-405). */
+int qvti_get_config(const qvti_sim* sim, qvti_config* cfg);
+
+/* Number of simulations qvti_create has made in this process (diagnostics:
+ * shows whether a shot loop allocates per shot).  No counterpart in the
+ * reference. */
+long long qvti_sims_created(void);
 
 /* Set the model: velp, vels, rho, gama_p = atan(1/Qp)/pi, gama_s (and eps,
  * delta when vti) as ntp floats each, host pointers (on_device = 0) or device
@@ -114,6 +127,16 @@ int qvti_device_field(qvti_sim* sim, int which, float** dev_ptr);
 /* Sum of squares of every wavefield (FP64 reduction on the device): the
  * per-run energy-norm check; also flags non-finite values. */
 int qvti_field_norms(qvti_sim* sim, double* norms9, int* nonfinite);
+
+/* Non-finite sentinel: queue, on the simulation's stream, a check of the
+ * particle velocities (a NaN or Inf anywhere reaches them within a step:
+ * every derivative is a global transform).  A hit sets a device flag that
+ * stays set until qvti_reset; when host_flag is not NULL (pinned host memory)
+ * the flag is copied there in stream order, so it is valid once work queued
+ * after this call has completed.  Asynchronous; the scheduler runs it after
+ * every chunk of steps and ends a shot with QVTI_ERR_NONFINITE.  The
+ * reference checks nothing (cuviscoelas_3D.cu:1255-1630). */
+int qvti_check_finite_async(qvti_sim* sim, int* host_flag);
 
 /* Checkpoint / resume.  A snapshot holds everything a step reads that an
  * earlier step wrote: particle velocities, stresses, the z-derivative
@@ -188,7 +211,6 @@ int qvti_q_derivative_noalloc(const float* d_in, float* d_out, int ntx, int nty,
  * around the whole program (viscoelas_3D.cpp:70-74, 472-480). */
 int qvti_profile_step(qvti_sim* sim, int nrep, int maxk, int* nkernels, char* names, float* ms, double* bytes);
 
-/* Last error code of this process and its description. */
 /* The simulation's CUDA stream (cudaStream_t), for callers that order their
  * own work after its steps.  The reference keeps one stream per device
  * inside struct MultiGPU (cuviscoelas_3D.cu:1168). */
@@ -197,6 +219,18 @@ int qvti_get_stream(qvti_sim* sim, void** stream);
 /* kz planes per batch of the k-space passes (1..nz/2+1); a tuning knob for
  * qvti_autotune.  No counterpart in the reference. */
 int qvti_set_kz_batch(qvti_sim* sim, int kz_batch);
+
+/* Form of the transforms.  QVTI_FORM_PLAIN: every FFT stage as FP32
+ * butterflies.  QVTI_FORM_TC: the 256-point y transforms (forward and
+ * inverse, the reference's cufftExecC2C work of cuviscoelas_3D.cu:1272-1562
+ * along y) as split-precision tensor-core contractions -- each radix-16
+ * stage a 16-point DFT matrix product on tcgen05 with TF32 hi/lo operands
+ * (three products, FP32 accumulation); the other transforms stay FP32.
+ * QVTI_ERR_UNSUPPORTED when the grid's y length is not 256.  A device-side
+ * wait that times out makes the next qvti_sync / qvti_get_records return
+ * QVTI_ERR_TIMEOUT.  No counterpart in the reference. */
+enum { QVTI_FORM_PLAIN = 0, QVTI_FORM_TC = 1 };
+int qvti_set_form(qvti_sim* sim, int form);
 
 /* ---------------------------------------------------------------------
  * Batches and serving.  The reference runs shots one after another from a
@@ -267,6 +301,7 @@ int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_opts* opts, q
 int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active, int* best_kz_batch,
                   double* gcell_steps);
 
+/* Last error code of the calling thread and its description. */
 int qvti_last_error(void);
 const char* qvti_error_string(int code);
 

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <vector>
@@ -13,19 +14,29 @@
 #include "../../include/qvti.h"
 
 namespace qvti {
-namespace {
 
 thread_local int g_last_error = QVTI_OK;
-std::mutex g_err_mu;
-int g_last_error_global = QVTI_OK;
 
 int fail(int code)
 {
     g_last_error = code;
-    std::lock_guard<std::mutex> lk(g_err_mu);
-    g_last_error_global = code;
     return code;
 }
+
+// Kernel attributes (the large dynamic shared-memory limits) are per device:
+// each device is configured once, the first time a simulation or a stage
+// entry point uses it, with that device current.
+namespace {
+PerDeviceOnce<kMaxDevices> g_configured;
+std::atomic<long long> g_sims_created{0};
+}  // namespace
+
+int configure_device(int dev)
+{
+    return g_configured.run(dev, [] { return configure_kernels(); });
+}
+
+namespace {
 
 #define QV_CUDA(call)                                                                        \
     do {                                                                                     \
@@ -78,7 +89,8 @@ bool make_plan(int n, FftPlan* p)
 // its real part -- the Hermitian part of the multiplier, which is what the
 // real part of the reference's C2C output sees; C-PML a, b (cu:213-309,
 // velp_max forced to 5000, R = 1e-2, pi = 3.1415926) and their half-point
-// averages 0.5 (v[i] + v[i+1]).
+// averages 0.5 (v[i] + v[i+1]); with a == nullptr the C-PML outputs are not
+// written (a, b, ah, bh may all be null then).
 __global__ void k_axis_tables(int n, double d, double f0, int pml, float2* tw, float* kmag, float2* F, float2* B,
                               float* a, float* b, float* ah, float* bh)
 {
@@ -97,6 +109,7 @@ __global__ void k_axis_tables(int n, double d, double f0, int pml, float2* tw, f
         if (2 * i == n) { fi = 0.0; bi = 0.0; }
         F[i] = make_float2((float)fr, (float)fi);
         B[i] = make_float2((float)br, (float)bi);
+        if (!a) continue;  // no C-PML profiles wanted (spectral stages only)
         auto prof = [&](int j, double* av, double* bv) {
             const double alpha_max = pi_ref * f0;
             const double om_max = 4.0 * 5000.0 * log(1.0 / (double)1e-2f) / (2.0 * pml * d);
@@ -139,6 +152,23 @@ __global__ void k_norms(long long ntp, const float* f, double* out, int* nonfini
     if (threadIdx.x == 0 && bad) atomicOr(nonfinite, 1);
 }
 
+// Any non-finite value among 4 n4 floats of each of three fields sets *flag
+// (float4 loads; every grid axis is even, so ntp is a multiple of 4).  x * 0
+// is +-0 for finite x and NaN for Inf or NaN, so a sum of such products is
+// zero exactly when every value is finite (a sum of the values themselves
+// could overflow).
+__global__ void k_finite3(long long n4, const float4* a, const float4* b, const float4* c, int* flag)
+{
+    int bad = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        const float4 x = a[i], y = b[i], z = c[i];
+        const float s = (x.x * 0.f + x.y * 0.f + x.z * 0.f + x.w * 0.f) + (y.x * 0.f + y.y * 0.f + y.z * 0.f + y.w * 0.f) +
+                        (z.x * 0.f + z.y * 0.f + z.z * 0.f + z.w * 0.f);
+        bad |= !(s == 0.f);
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
 }  // namespace
 
 bool make_fft_plan(int n, FftPlan* p) { return make_plan(n, p); }
@@ -165,6 +195,8 @@ struct Sim {
     size_t rik_cap = 0, rix_cap = 0, rec_cap = 0;  // element capacities of the buffers above
     double* d_norm = nullptr;
     int* d_bad = nullptr;
+    int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
+    int* d_nonfinite = nullptr;  // set by qvti_check_finite_async
     int nt = 0, rn = 0;
     bool have_model = false, have_src = false;
     int steps = 0;
@@ -215,9 +247,38 @@ struct Sim {
 
 namespace {
 
-// Number of full-grid float arrays and half-spectrum complex arrays.
-constexpr int kRealArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6 + 12 + 5 + 3;
+// A device buffer freed when it goes out of scope (error returns included).
+struct DevBuf {
+    void* p = nullptr;
+    float* f() const { return static_cast<float*>(p); }
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+// Number of full-grid float arrays (v, s, R, Q, coefficients, MU, 1/rho),
+// of C-PML slab arrays per axis (x, y, z) and of half-spectrum complex arrays.
+constexpr int kRealArrays = 3 + 6 + 3 + 6 + 12 + 5 + 3;
+constexpr int kSlabArrays[3] = {13, 13, 11};  // php 3/3/3, phn 3/3/2, qn 3/3/2, phs 2/2/2, qs 2/2/2
 constexpr int kSpecArrays = 3 + 3 + 3 + kNumGxy;  // H, Hy, Yv, G without the one-axis fields
+
+// Every C-PML slab array of a simulation with its length in floats.
+int slab_arrays(const KP& k, float** out, size_t* len)
+{
+    int n = 0;
+    auto add = [&](float* p, int axis) {
+        out[n] = p;
+        len[n++] = (size_t)slab_len(k.nx, k.ny, k.nz, k.pml, axis);
+    };
+    for (int c = 0; c < 9; ++c) add(k.php[c], c % 3);
+    for (int c = 0; c < 8; ++c) add(k.phn[c], c < 3 ? 0 : c < 6 ? 1 : 2);
+    for (int c = 0; c < 8; ++c) add(k.qn[c], c < 3 ? 0 : c < 6 ? 1 : 2);
+    for (int c = 0; c < 6; ++c) add(k.phs[c], kPhsAxis[c]);
+    for (int c = 0; c < 6; ++c) add(k.qs[c], kPhsAxis[c]);
+    return n;
+}
+constexpr int kNumSlab = 9 + 8 + 8 + 6 + 6;
 
 int build_graph(Sim* s)
 {
@@ -240,12 +301,14 @@ using qvti::fail;
 
 struct qvti_sim : qvti::Sim {};
 
-extern "C" size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int vti)
+extern "C" size_t qvti_footprint_bytes(int ntx, int nty, int ntz, int pml, int vti)
 {
     (void)vti;
     const size_t ntp = (size_t)ntx * nty * ntz;
     const size_t nspec = (size_t)(ntz / 2 + 1) * ntx * nty;
-    return ntp * sizeof(float) * qvti::kRealArrays + nspec * sizeof(float2) * qvti::kSpecArrays;
+    size_t slab = 0;
+    for (int a = 0; a < 3; ++a) slab += (size_t)qvti::kSlabArrays[a] * (size_t)qvti::slab_len(ntx, nty, ntz, pml, a);
+    return ntp * sizeof(float) * qvti::kRealArrays + slab * sizeof(float) + nspec * sizeof(float2) * qvti::kSpecArrays;
 }
 
 extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
@@ -263,10 +326,7 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     if (!make_plan(nx, &px) || !make_plan(ny, &py) || !make_plan(nz, &pz)) return fail(QVTI_ERR_UNSUPPORTED);
 
     QV_CUDA(cudaSetDevice(cfg->device));
-    static std::once_flag once;
-    static int cfg_err = 0;
-    std::call_once(once, [] { cfg_err = configure_kernels(); });
-    if (cfg_err) return fail(QVTI_ERR_CUDA);
+    if (configure_device(cfg->device)) return fail(QVTI_ERR_CUDA);
 
     Sim* s = new (std::nothrow) qvti_sim();
     if (!s) return fail(QVTI_ERR_OOM);
@@ -314,11 +374,14 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.s[c], ntp);
     for (int c = 0; c < 3; ++c) rc |= s->alloc(&k.R[c], ntp);
     for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.Q[c], ntp);
-    for (int c = 0; c < 9; ++c) rc |= s->alloc(&k.php[c], ntp);
-    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.phn[c], ntp);
-    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.qn[c], ntp);
-    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.phs[c], ntp);
-    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.qs[c], ntp);
+    // C-PML memory variables: slab storage (engine.cuh, slab_x/y/z)
+    const int pml = cfg->pml;
+    auto slab = [&](int axis) { return (size_t)slab_len(nx, ny, nz, pml, axis); };
+    for (int c = 0; c < 9; ++c) rc |= s->alloc(&k.php[c], slab(c % 3));
+    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.phn[c], slab(c < 3 ? 0 : c < 6 ? 1 : 2));
+    for (int c = 0; c < 8; ++c) rc |= s->alloc(&k.qn[c], slab(c < 3 ? 0 : c < 6 ? 1 : 2));
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.phs[c], slab(kPhsAxis[c]));
+    for (int c = 0; c < 6; ++c) rc |= s->alloc(&k.qs[c], slab(kPhsAxis[c]));
     if (rc) return bail(g_last_error);
     float* mu[5];
     float* rinv[3];
@@ -338,7 +401,19 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     rc |= s->alloc(&s->d_it, 1);
     rc |= s->alloc(&s->d_norm, 16);
     rc |= s->alloc(&s->d_bad, 4);
+    rc |= s->alloc(&s->d_err, 1);
+    rc |= s->alloc(&s->d_nonfinite, 1);
+    float* dft16 = nullptr;
+    rc |= s->alloc(&dft16, 4096);
     if (rc) return bail(g_last_error);
+    launch_dft16_tables(dft16, s->st);
+    if (cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st) != cudaSuccess ||
+        cudaMemsetAsync(s->d_nonfinite, 0, sizeof(int), s->st) != cudaSuccess)
+        return bail(QVTI_ERR_CUDA);
+    k.dft16 = dft16;
+    k.err = s->d_err;
+    k.form = kFormPlain;
+
     for (int j = 0; j < 5; ++j) k.MU[j] = mu[j];
     k.mrho = s->coef[0]; k.mgp = s->coef[1]; k.mgs = s->coef[2];
     k.mc33 = s->coef[4]; k.mcs = s->coef[6];
@@ -363,6 +438,16 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     for (int c = 0; c < 3; ++c) k.rec[c] = nullptr;
     if (cudaStreamSynchronize(s->st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return bail(QVTI_ERR_CUDA);
     *out = static_cast<qvti_sim*>(s);
+    g_sims_created.fetch_add(1);
+    return QVTI_OK;
+}
+
+extern "C" long long qvti_sims_created(void) { return qvti::g_sims_created.load(); }
+
+extern "C" int qvti_get_config(const qvti_sim* s, qvti_config* cfg)
+{
+    if (!s || !cfg) return fail(QVTI_ERR_ARG);
+    *cfg = s->cfg;
     return QVTI_OK;
 }
 
@@ -500,13 +585,14 @@ extern "C" int qvti_reset(qvti_sim* s)
     for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.s[c], 0, b, s->st));
     for (int c = 0; c < 3; ++c) QV_CUDA(cudaMemsetAsync(k.R[c], 0, b, s->st));
     for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.Q[c], 0, b, s->st));
-    for (int c = 0; c < 9; ++c) QV_CUDA(cudaMemsetAsync(k.php[c], 0, b, s->st));
-    for (int c = 0; c < 8; ++c) QV_CUDA(cudaMemsetAsync(k.phn[c], 0, b, s->st));
-    for (int c = 0; c < 8; ++c) QV_CUDA(cudaMemsetAsync(k.qn[c], 0, b, s->st));
-    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.phs[c], 0, b, s->st));
-    for (int c = 0; c < 6; ++c) QV_CUDA(cudaMemsetAsync(k.qs[c], 0, b, s->st));
+    float* sl[kNumSlab];
+    size_t sn[kNumSlab];
+    slab_arrays(k, sl, sn);
+    for (int c = 0; c < kNumSlab; ++c) QV_CUDA(cudaMemsetAsync(sl[c], 0, sizeof(float) * sn[c], s->st));
     const int minus1 = -1;
     QV_CUDA(cudaMemcpyAsync(s->d_it, &minus1, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    QV_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st));
+    QV_CUDA(cudaMemsetAsync(s->d_nonfinite, 0, sizeof(int), s->st));
     for (int c = 0; c < 3; ++c)
         if (s->d_rec[c]) QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * s->rn, s->st));
     QV_CUDA(cudaStreamSynchronize(s->st));
@@ -549,13 +635,24 @@ extern "C" int qvti_step_timed(qvti_sim* s, int nsteps, float* ms)
     return QVTI_OK;
 }
 
+namespace qvti {
+// After the simulation's stream is idle: a kernel that gave up a bounded wait
+// left a status in the device error flag.
+int device_status(Sim* s)
+{
+    int e = 0;
+    QV_CUDA(cudaMemcpy(&e, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return e ? fail(e) : QVTI_OK;
+}
+}  // namespace qvti
+
 extern "C" int qvti_sync(qvti_sim* s)
 {
     using namespace qvti;
     if (!s) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     QV_CUDA(cudaStreamSynchronize(s->st));
-    return QVTI_OK;
+    return device_status(s);
 }
 
 extern "C" int qvti_steps_done(const qvti_sim* s) { return s ? s->steps : -1; }
@@ -570,7 +667,7 @@ extern "C" int qvti_get_records(qvti_sim* s, float* vx, float* vy, float* vz)
     const size_t n = (size_t)s->steps * s->rn;
     for (int c = 0; c < 3; ++c)
         if (dst[c] && n && s->d_rec[c]) QV_CUDA(cudaMemcpy(dst[c], s->d_rec[c], n * sizeof(float), cudaMemcpyDeviceToHost));
-    return QVTI_OK;
+    return device_status(s);
 }
 
 static float* field_ptr(qvti_sim* s, int which)
@@ -599,6 +696,20 @@ extern "C" int qvti_device_field(qvti_sim* s, int which, float** p)
     return QVTI_OK;
 }
 
+extern "C" int qvti_check_finite_async(qvti_sim* s, int* host_flag)
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    k_finite3<<<148 * 4, 256, 0, s->st>>>(s->ntp / 4, reinterpret_cast<const float4*>(s->kp.v[0]),
+                                          reinterpret_cast<const float4*>(s->kp.v[1]),
+                                          reinterpret_cast<const float4*>(s->kp.v[2]), s->d_nonfinite);
+    QV_CUDA(cudaGetLastError());
+    if (host_flag)
+        QV_CUDA(cudaMemcpyAsync(host_flag, s->d_nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    return QVTI_OK;
+}
+
 extern "C" int qvti_field_norms(qvti_sim* s, double* norms9, int* nonfinite)
 {
     using namespace qvti;
@@ -624,8 +735,9 @@ extern "C" int qvti_field_norms(qvti_sim* s, double* norms9, int* nonfinite)
 // ------------------------------------------------------ checkpoint / resume --
 namespace {
 
-// Snapshot layout: this header, then kStateArrays full-grid float arrays in
-// state_arrays() order, then the records of the steps done (vx, vy, vz, each
+// Snapshot layout: this header, then kStateArrays float arrays in
+// state_arrays() order (18 full-grid arrays, then the 37 C-PML slab arrays,
+// each its own length), then the records of the steps done (vx, vy, vz, each
 // [step][receiver]).  Grid, spacing, dt, C-PML width and medium type are in
 // the header so a snapshot cannot resume a different simulation.
 struct StateHeader {
@@ -633,29 +745,28 @@ struct StateHeader {
     int32_t ntx, nty, ntz, pml;
     int32_t vti, n_arrays, steps, rn;
     float dx, dy, dz, dt;
-    uint64_t array_bytes, total_bytes;
+    uint64_t array_bytes, total_bytes;  // all state arrays together; the whole snapshot
 };
 static_assert(sizeof(StateHeader) == 72, "snapshot header layout");
-constexpr char kStateMagic[8] = {'Q', 'V', 'T', 'I', 'S', 'T', '0', '1'};
-constexpr int kStateArrays = 3 + 6 + 3 + 6 + 9 + 8 + 8 + 6 + 6;
+constexpr char kStateMagic[8] = {'Q', 'V', 'T', 'I', 'S', 'T', '0', '2'};
+constexpr int kStateArrays = 3 + 6 + 3 + 6 + qvti::kNumSlab;
 
-int state_arrays(Sim* s, float** out)
+int state_arrays(Sim* s, float** out, size_t* bytes)
 {
     qvti::KP& k = s->kp;
     int n = 0;
-    for (float* p : k.v) out[n++] = p;
-    for (float* p : k.s) out[n++] = p;
-    for (float* p : k.R) out[n++] = p;
-    for (float* p : k.Q) out[n++] = p;
-    for (float* p : k.php) out[n++] = p;
-    for (float* p : k.phn) out[n++] = p;
-    for (float* p : k.qn) out[n++] = p;
-    for (float* p : k.phs) out[n++] = p;
-    for (float* p : k.qs) out[n++] = p;
-    return n;
+    const size_t full = sizeof(float) * (size_t)s->ntp;
+    for (float* p : k.v) { out[n] = p; bytes[n++] = full; }
+    for (float* p : k.s) { out[n] = p; bytes[n++] = full; }
+    for (float* p : k.R) { out[n] = p; bytes[n++] = full; }
+    for (float* p : k.Q) { out[n] = p; bytes[n++] = full; }
+    size_t len[qvti::kNumSlab];
+    const int ns = qvti::slab_arrays(k, out + n, len);
+    for (int i = 0; i < ns; ++i) bytes[n + i] = sizeof(float) * len[i];
+    return n + ns;
 }
 
-StateHeader state_header(const Sim* s)
+StateHeader state_header(Sim* s)
 {
     StateHeader h{};
     memcpy(h.magic, kStateMagic, sizeof(h.magic));
@@ -665,9 +776,13 @@ StateHeader state_header(const Sim* s)
     h.steps = s->steps;
     h.rn = s->rn;
     h.dx = s->cfg.dx; h.dy = s->cfg.dy; h.dz = s->cfg.dz; h.dt = s->cfg.dt;
-    h.array_bytes = sizeof(float) * (uint64_t)s->ntp;
+    float* arr[kStateArrays];
+    size_t b[kStateArrays];
+    state_arrays(s, arr, b);
+    h.array_bytes = 0;
+    for (size_t x : b) h.array_bytes += x;
     const uint64_t rec = s->rn > 0 && s->d_rec[0] ? 3ull * s->steps * s->rn * sizeof(float) : 0;
-    h.total_bytes = sizeof(StateHeader) + h.array_bytes * kStateArrays + rec;
+    h.total_bytes = sizeof(StateHeader) + h.array_bytes + rec;
     return h;
 }
 
@@ -691,13 +806,14 @@ extern "C" int qvti_save_state(qvti_sim* s, void* host, size_t bytes)
     memcpy(dst, &h, sizeof(h));
     dst += sizeof(h);
     float* arr[kStateArrays];
-    state_arrays(s, arr);
-    for (float* p : arr) {
-        QV_CUDA(cudaMemcpyAsync(dst, p, h.array_bytes, cudaMemcpyDeviceToHost, s->st));
-        dst += h.array_bytes;
+    size_t ab[kStateArrays];
+    state_arrays(s, arr, ab);
+    for (int i = 0; i < kStateArrays; ++i) {
+        QV_CUDA(cudaMemcpyAsync(dst, arr[i], ab[i], cudaMemcpyDeviceToHost, s->st));
+        dst += ab[i];
     }
     const size_t rec = sizeof(float) * (size_t)h.steps * h.rn;
-    if (h.total_bytes > sizeof(h) + h.array_bytes * kStateArrays)
+    if (h.total_bytes > sizeof(h) + h.array_bytes)
         for (int c = 0; c < 3; ++c) {
             QV_CUDA(cudaMemcpyAsync(dst, s->d_rec[c], rec, cudaMemcpyDeviceToHost, s->st));
             dst += rec;
@@ -721,15 +837,16 @@ extern "C" int qvti_load_state(qvti_sim* s, const void* host, size_t bytes)
     if (!same || h.steps < 0 || h.steps > s->nt || h.rn != s->rn) return fail(QVTI_ERR_ARG);
     const uint64_t rec = sizeof(float) * (uint64_t)h.steps * h.rn;
     const bool with_rec = h.rn > 0 && s->d_rec[0];
-    const uint64_t want = sizeof(h) + h.array_bytes * kStateArrays + (with_rec ? 3 * rec : 0);
+    const uint64_t want = sizeof(h) + h.array_bytes + (with_rec ? 3 * rec : 0);
     if (h.total_bytes != want || bytes < want) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     const char* src = static_cast<const char*>(host) + sizeof(h);
     float* arr[kStateArrays];
-    state_arrays(s, arr);
-    for (float* p : arr) {
-        QV_CUDA(cudaMemcpyAsync(p, src, h.array_bytes, cudaMemcpyHostToDevice, s->st));
-        src += h.array_bytes;
+    size_t ab[kStateArrays];
+    state_arrays(s, arr, ab);
+    for (int i = 0; i < kStateArrays; ++i) {
+        QV_CUDA(cudaMemcpyAsync(arr[i], src, ab[i], cudaMemcpyHostToDevice, s->st));
+        src += ab[i];
     }
     if (with_rec) {
         const size_t all = sizeof(float) * (size_t)s->nt * s->rn;
@@ -766,17 +883,15 @@ extern "C" int qvti_derivative_1d(qvti_sim* s, int axis, int fwd, const float* i
     using namespace qvti;
     if (!s || !in || !out || axis < 0 || axis > 2) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
-    float *din = nullptr, *dout = nullptr;
     const size_t b = sizeof(float) * s->ntp;
-    QV_CUDA(cudaMalloc(&din, b));
-    QV_CUDA(cudaMalloc(&dout, b));
-    QV_CUDA(cudaMemcpyAsync(din, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
-    launch_derivative_1d(s->kp, axis, fwd, din, dout, s->st);
+    DevBuf din, dout;  // freed on every return
+    QV_CUDA(cudaMalloc(&din.p, b));
+    QV_CUDA(cudaMalloc(&dout.p, b));
+    QV_CUDA(cudaMemcpyAsync(din.p, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
+    launch_derivative_1d(s->kp, axis, fwd, din.f(), dout.f(), s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
-    QV_CUDA(cudaMemcpy(out, dout, b, cudaMemcpyDeviceToHost));
-    cudaFree(din);
-    cudaFree(dout);
+    QV_CUDA(cudaMemcpy(out, dout.p, b, cudaMemcpyDeviceToHost));
     return QVTI_OK;
 }
 
@@ -854,21 +969,19 @@ extern "C" int qvti_q_derivative(qvti_sim* s, int axis, int fwd, int power, cons
     if (!s || !in || !out || axis < 0 || axis > 2 || power < -1 || power > 1) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     QV_CUDA(cudaStreamSynchronize(s->st));
-    float *din = nullptr, *dout = nullptr;
     const size_t b = sizeof(float) * s->ntp;
-    QV_CUDA(cudaMalloc(&din, b));
-    QV_CUDA(cudaMalloc(&dout, b));
-    QV_CUDA(cudaMemcpyAsync(din, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
+    DevBuf din, dout;  // freed on every return
+    QV_CUDA(cudaMalloc(&din.p, b));
+    QV_CUDA(cudaMalloc(&dout.p, b));
+    QV_CUDA(cudaMemcpyAsync(din.p, in, b, cudaMemcpyHostToDevice, s->st));  // ordered before the launches
     KP k = s->kp;
-    k.v[0] = din;
+    k.v[0] = din.f();
     k.H[0] = s->kp.G[0];  // scratch: rewritten by every time step anyway
     k.G[0] = s->kp.G[0];
-    launch_q_derivative(k, axis, fwd, power, dout, s->st);
+    launch_q_derivative(k, axis, fwd, power, dout.f(), s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
-    QV_CUDA(cudaMemcpy(out, dout, b, cudaMemcpyDeviceToHost));
-    cudaFree(din);
-    cudaFree(dout);
+    QV_CUDA(cudaMemcpy(out, dout.p, b, cudaMemcpyDeviceToHost));
     return QVTI_OK;
 }
 
@@ -885,6 +998,20 @@ extern "C" int qvti_set_kz_batch(qvti_sim* s, int kz_batch)
     if (!s || kz_batch < 1 || kz_batch > s->nkz) return fail(QVTI_ERR_ARG);
     if (s->kp.kz_batch != kz_batch) {
         s->kp.kz_batch = kz_batch;
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_form(qvti_sim* s, int form)
+{
+    using namespace qvti;
+    if (!s || (form != QVTI_FORM_PLAIN && form != QVTI_FORM_TC)) return fail(QVTI_ERR_ARG);
+    KP probe = s->kp;
+    probe.form = form == QVTI_FORM_TC ? kFormTc : kFormPlain;
+    if (form == QVTI_FORM_TC && !tc_cy_available(probe)) return fail(QVTI_ERR_UNSUPPORTED);
+    if (s->kp.form != probe.form) {
+        s->kp.form = probe.form;
         if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     }
     return QVTI_OK;

@@ -12,9 +12,9 @@
 //              reference's spectral time derivative (V - Vprev)/dt
 //              (cuviscoelas_3D.cu:514-531) becomes (Q - Qprev)/dt by
 //              linearity, saving 18 of its 45 inverse transforms    float
-//   C-PML      memory variables and per-term loss potentials, allocated
-//              full size but read/written only inside their axis slab
-//              (they are identically zero elsewhere, b = 0 there)   float
+//   C-PML      memory variables and per-term loss potentials, stored for
+//              their axis slab only (they are identically zero elsewhere,
+//              b = 0 there; see slab_x/slab_y/slab_z)               float
 //   coef       rho, gamma_p, gamma_s and the effective velocities of c11,
 //              c33, c13, c44 (7; 5 distinct when isotropic), MU (5, the
 //              8-point averaged shear set), 1/rho-bar per velocity component;
@@ -32,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include "fft.cuh"
+#include "per_device.h"
 
 namespace qvti {
 
@@ -45,6 +46,16 @@ constexpr int kNumG = 27;
 constexpr int kNumGxy = kNumG - 6;  // fields that go through k_mx and k_cy
 __host__ __device__ constexpr bool is_gz(int o) { return o == 7 || o == 10 || o == 22; }
 __host__ __device__ constexpr bool is_gy(int o) { return o == 4 || o == 16 || o == 25; }
+// G index of the c-th field that goes through the x and y passes.
+__host__ __device__ inline int gxy_field(int c)
+{
+    int o = -1;
+    for (int n = 0; n <= c;) {
+        ++o;
+        if (!is_gz(o) && !is_gy(o)) ++n;
+    }
+    return o;
+}
 
 struct KP {
     int nx, ny, nz, nkz, pml;
@@ -90,7 +101,43 @@ struct KP {
     float* rec[3];
     int* d_it;       // current step index, advanced on the device each step
     int kz_batch;    // kz planes per batch of the k-space passes
+    // form of the transforms: kFormPlain (FP32 butterflies) or kFormTc (the
+    // 256-point y transforms as split-precision tensor-core contractions)
+    int form;
+    const float* dft16;  // tensor-core DFT matrices (k_dft16_tables), null if unused
+    int* err;            // device error flag (a bounded wait that gave up), 0 = ok
 };
+constexpr int kFormPlain = 0, kFormTc = 1;
+
+// C-PML memory variables are non-zero only inside their axis' slabs (b = 0
+// elsewhere, cuviscoelas_3D.cu:291-307), so each is stored for the 2 pml
+// planes of its axis only: x-slab [2 pml][ny][nz], y-slab [nx][2 pml][nz],
+// z-slab [nx][ny][2 pml], the slab coordinate xs = x for x < pml and
+// x - (nx - 2 pml) for x >= nx - pml.  Axis of each variable: php[m] m % 3
+// (x, y, z); phn[m], qn[m]: m < 3 x, m < 6 y, else z; phs[m], qs[m]:
+// {z, x, y, x, z, y}.
+__device__ __forceinline__ int slab_x(const KP& k, int x, int y, int z)
+{
+    const int xs = x < k.pml ? x : x - k.nx + 2 * k.pml;
+    return (xs * k.ny + y) * k.nz + z;
+}
+__device__ __forceinline__ int slab_y(const KP& k, int x, int y, int z)
+{
+    const int ys = y < k.pml ? y : y - k.ny + 2 * k.pml;
+    return (x * 2 * k.pml + ys) * k.nz + z;
+}
+__device__ __forceinline__ int slab_z(const KP& k, int x, int y, int z)
+{
+    const int zs = z < k.pml ? z : z - k.nz + 2 * k.pml;
+    return (x * k.ny + y) * 2 * k.pml + zs;
+}
+constexpr int kPhsAxis[6] = {2, 0, 1, 0, 2, 1};
+// Floats in the slab of `axis` (0 x, 1 y, 2 z).
+inline long long slab_len(int nx, int ny, int nz, int pml, int axis)
+{
+    const long long t = 2ll * pml;
+    return axis == 0 ? t * ny * nz : axis == 1 ? (long long)nx * t * nz : (long long)nx * ny * t;
+}
 
 // Host-side launchers (step_kernels.cu).  All launch on `st`.
 constexpr int kStepKernels = 8;
@@ -112,11 +159,23 @@ void launch_coef_build(const KP& kp, const float* velp, const float* vels, const
                        float w0, float* const* coef_out, cudaStream_t st);
 void launch_mu_rinv(const KP& kp, const float* rho, const float* const* sset, cudaStream_t st);
 int configure_kernels();   // raise dynamic shared-memory limits, returns cudaError_t
+// configure_kernels() once per device (the device must be current); 0 = ok.
+int configure_device(int dev);
+// Record `code` as the calling thread's last error (qvti_last_error) and
+// return it.
+int fail(int code);
 
 // Radix plan of a transform length; FP64 build of one axis's 1D tables.
 bool make_fft_plan(int n, FftPlan* p);
 void launch_axis_tables(int n, double d, double f0, int pml, float2* tw, float* kmag, float2* F, float2* B,
                         float* a, float* b, float* ah, float* bh, cudaStream_t st);
+
+// Tensor-core form (tc_dft.cu): 256-point y transforms on tcgen05.
+bool tc_cy_available(const KP& k);
+size_t tc_cy_smem();
+int configure_tc_kernels();
+void launch_dft16_tables(float* out, cudaStream_t st);  // 4096 floats
+void launch_cy_tc(const KP& k, bool inv, int nfield, long long line0, long long line_end, cudaStream_t st);
 
 // Individual stages, exposed for unit tests through the C ABI.
 void launch_q_derivative(const KP& kp, int axis, int fwd, int pw, float* out, cudaStream_t st);

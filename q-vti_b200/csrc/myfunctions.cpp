@@ -17,7 +17,8 @@ extern "C" void getdevice(int* GPU_N)
 
 // Allocation needs the grid only; the engine itself is created on the first
 // shot, when pml, spacing, dt and f0 are known (the reference passes them to
-// cuda_forward_acoustic_3D, not to cuda_Device_malloc).
+// cuda_forward_acoustic_3D, not to cuda_Device_malloc), and kept for the
+// following shots while those stay the same.
 extern "C" void cuda_Device_malloc(int ntx, int nty, int ntz, int ntp, int nx, int ny, int nz, int nt, int rnmax,
                                    struct MultiGPU plan[], int GPU_N)
 {
@@ -44,6 +45,15 @@ extern "C" void cuda_Host_initialization(int ntp, int nt, int rnmax, struct Mult
     }
 }
 
+namespace {
+// Everything qvti_create fixes: the same values let a simulation run the next shot.
+bool same_engine(const qvti_config& a, const qvti_config& b)
+{
+    return a.ntx == b.ntx && a.nty == b.nty && a.ntz == b.ntz && a.pml == b.pml && a.dx == b.dx && a.dy == b.dy &&
+           a.dz == b.dz && a.dt == b.dt && a.f0 == b.f0 && a.w0 == b.w0 && a.vti == b.vti && a.device == b.device;
+}
+}  // namespace
+
 extern "C" void cuda_forward_acoustic_3D(int myid, int is, int nt, int ntx, int nty, int ntz, int ntp, int nx,
                                          int ny, int nz, int pml, float dx, float dy, float dz, float dt, float f0,
                                          float w0, float velp_max, float* rik, float* velp, float* gama_p,
@@ -58,16 +68,23 @@ extern "C" void cuda_forward_acoustic_3D(int myid, int is, int nt, int ntx, int 
     for (int i = 0; i < GPU_N; ++i) {
         MultiGPU& p = plan[i];
         const Source& s = ss[is + i];
-        if (p.sim) {
-            qvti_destroy(p.sim);
-            p.sim = nullptr;
-        }
         qvti_config cfg;
         std::memset(&cfg, 0, sizeof(cfg));
         cfg.ntx = ntx; cfg.nty = nty; cfg.ntz = ntz; cfg.pml = pml;
         cfg.dx = dx; cfg.dy = dy; cfg.dz = dz; cfg.dt = dt; cfg.f0 = f0; cfg.w0 = w0;
         cfg.vti = 0; cfg.device = i;
-        if (qvti_create(&cfg, &p.sim)) continue;
+        // the engine allocated for the previous shot is kept when this shot
+        // has the same grid and constants (the reference allocates once in
+        // cuda_Device_malloc and reuses its buffers for every shot,
+        // viscoelas_3D.cpp:355-405); model, source and receivers are set again
+        if (p.sim) {
+            qvti_config have;
+            if (qvti_get_config(p.sim, &have) || !same_engine(have, cfg)) {
+                qvti_destroy(p.sim);
+                p.sim = nullptr;
+            }
+        }
+        if (!p.sim && qvti_create(&cfg, &p.sim)) continue;
         if (qvti_set_model(p.sim, velp, vels, rho, gama_p, gama_s, nullptr, nullptr, 0)) continue;
         if (qvti_set_receivers(p.sim, s.r_iz, s.r_ix, s.r_iy, rn)) continue;
         if (qvti_set_source(p.sim, QVTI_SRC_FORCE_X, s.s_ix, s.s_iy, s.s_iz + 10, rik, nt)) continue;

@@ -30,7 +30,6 @@ static __device__ __align__(256) float2 g_na_tw[3][kNoAllocAxis];
 static __device__ __align__(256) float2 g_na_F[3][kNoAllocAxis];
 static __device__ __align__(256) float2 g_na_B[3][kNoAllocAxis];
 static __device__ __align__(256) float g_na_k[3][kNoAllocAxis];
-static __device__ __align__(256) float g_na_pml[3][4][kNoAllocAxis];
 
 // Device addresses of the arrays above, looked up once per device with that
 // device current (a host-side use of the array names would not be a device
@@ -38,9 +37,8 @@ static __device__ __align__(256) float g_na_pml[3][4][kNoAllocAxis];
 struct NoAllocDev {
     bool ready = false;
     float2 *scratch = nullptr, *tw = nullptr, *F = nullptr, *B = nullptr;
-    float *k = nullptr, *pml = nullptr;
+    float* k = nullptr;
 };
-constexpr int kMaxDevices = 64;
 NoAllocDev g_na_dev[kMaxDevices];
 std::mutex g_na_mu;
 
@@ -60,12 +58,11 @@ int setup_device(int dev, NoAllocDev** out)
         addr((void**)&d.F, g_na_F);
         addr((void**)&d.B, g_na_B);
         addr((void**)&d.k, g_na_k);
-        addr((void**)&d.pml, g_na_pml);
         if (e != cudaSuccess) {
             fprintf(stderr, "qvti_q_derivative_noalloc: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
             return QVTI_ERR_CUDA;
         }
-        if (configure_kernels() != 0) return QVTI_ERR_CUDA;  // shared-memory limits of this device
+        if (configure_device(dev) != 0) return QVTI_ERR_CUDA;  // shared-memory limits of this device
         d.ready = true;
     }
     *out = &d;
@@ -89,36 +86,34 @@ extern "C" int qvti_q_derivative_noalloc(const float* d_in, float* d_out, int nt
 {
     using namespace qvti;
     if (!d_in || !d_out || axis < 0 || axis > 2 || power < -1 || power > 1 || !(dx > 0 && dy > 0 && dz > 0))
-        return QVTI_ERR_ARG;
-    if (!smooth_even(ntx) || !smooth_even(nty) || !smooth_even(ntz)) return QVTI_ERR_UNSUPPORTED;
+        return fail(QVTI_ERR_ARG);
+    if (!smooth_even(ntx) || !smooth_even(nty) || !smooth_even(ntz)) return fail(QVTI_ERR_UNSUPPORTED);
     const long long nkz = ntz / 2 + 1;
     if (nkz * ntx * nty > kNoAllocSpectrum) {
         fprintf(stderr,
                 "qvti_q_derivative_noalloc: grid %dx%dx%d needs %lld spectrum values, the static scratch holds %lld\n",
                 ntx, nty, ntz, nkz * ntx * nty, kNoAllocSpectrum);
-        return QVTI_ERR_UNSUPPORTED;
+        return fail(QVTI_ERR_UNSUPPORTED);
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return QVTI_ERR_CUDA;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(QVTI_ERR_CUDA);
     NoAllocDev* d = nullptr;
     int rc = setup_device(dev, &d);
-    if (rc) return rc;
+    if (rc) return fail(rc);
 
     KP k{};
     k.nx = ntx; k.ny = nty; k.nz = ntz; k.nkz = (int)nkz; k.pml = 2;
     k.ntp = (long long)ntx * nty * ntz;
     k.inv_ntp = (float)(1.0 / (double)k.ntp);
     if (!make_fft_plan(ntx, &k.px) || !make_fft_plan(nty, &k.py) || !make_fft_plan(ntz, &k.pz))
-        return QVTI_ERR_UNSUPPORTED;
+        return fail(QVTI_ERR_UNSUPPORTED);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int n[3] = {ntx, nty, ntz};
     const float h[3] = {dx, dy, dz};
-    for (int a = 0; a < 3; ++a) {
-        float* pm = d->pml + (size_t)a * 4 * kNoAllocAxis;
+    for (int a = 0; a < 3; ++a)  // twiddles, |k| and shift multipliers; no C-PML profiles
         launch_axis_tables(n[a], h[a], 1.0, 2, d->tw + (size_t)a * kNoAllocAxis, d->k + (size_t)a * kNoAllocAxis,
-                           d->F + (size_t)a * kNoAllocAxis, d->B + (size_t)a * kNoAllocAxis, pm, pm + kNoAllocAxis,
-                           pm + 2 * kNoAllocAxis, pm + 3 * kNoAllocAxis, st);
-    }
+                           d->F + (size_t)a * kNoAllocAxis, d->B + (size_t)a * kNoAllocAxis, nullptr, nullptr,
+                           nullptr, nullptr, st);
     k.tw_x = d->tw; k.tw_y = d->tw + kNoAllocAxis; k.tw_z = d->tw + 2 * kNoAllocAxis;
     k.Fx = d->F; k.Fy = d->F + kNoAllocAxis; k.Fz = d->F + 2 * kNoAllocAxis;
     k.Bx = d->B; k.By = d->B + kNoAllocAxis; k.Bz = d->B + 2 * kNoAllocAxis;
@@ -130,7 +125,7 @@ extern "C" int qvti_q_derivative_noalloc(const float* d_in, float* d_out, int nt
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "qvti_q_derivative_noalloc: launch: %s\n", cudaGetErrorString(e));
-        return QVTI_ERR_CUDA;
+        return fail(QVTI_ERR_CUDA);
     }
     return QVTI_OK;
 }

@@ -98,6 +98,11 @@ struct PoolSim {
     size_t bytes = 0;
     bool busy = false;
     double last_used = 0;
+    int* nonfinite = nullptr;  // pinned host copy of the simulation's non-finite flag
+    ~PoolSim()
+    {
+        if (nonfinite) cudaFreeHost(nonfinite);
+    }
 };
 
 struct Job {
@@ -117,7 +122,7 @@ struct Job {
 
 size_t shot_bytes(const qvti_shot& s)
 {
-    return qvti_footprint_bytes(s.ntx, s.nty, s.ntz, s.vti) + 3 * sizeof(float) * (size_t)s.nt * (size_t)s.rn;
+    return qvti_footprint_bytes(s.ntx, s.nty, s.ntz, s.pml, s.vti) + 3 * sizeof(float) * (size_t)s.nt * (size_t)s.rn;
 }
 
 }  // namespace
@@ -217,7 +222,8 @@ PoolSim* qvti_server::acquire(const Job* j, bool* blocked)
     }
     auto ps = std::make_unique<PoolSim>();
     const qvti_config cfg = config_of(key, opts.device);
-    if (qvti_create(&cfg, &ps->sim) != QVTI_OK) {
+    if (cudaHostAlloc(reinterpret_cast<void**>(&ps->nonfinite), sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        qvti_create(&cfg, &ps->sim) != QVTI_OK) {
         std::lock_guard<std::mutex> lk(mu);
         pool_bytes = held;
         return nullptr;
@@ -246,6 +252,7 @@ int qvti_server::start(Job* j, PoolSim* ps)
     if ((rc = qvti_set_receivers(sim, s.r_iz, s.r_ix, s.r_iy, s.rn))) return rc;
     if ((rc = qvti_set_source(sim, s.src_type, s.s_ix, s.s_iy, s.s_iz, s.wavelet, s.nt))) return rc;
     if ((rc = qvti_reset(sim))) return rc;
+    *ps->nonfinite = 0;
     void* stv = nullptr;
     if ((rc = qvti_get_stream(sim, &stv))) return rc;
     j->st = static_cast<cudaStream_t>(stv);
@@ -260,7 +267,10 @@ int qvti_server::start(Job* j, PoolSim* ps)
     return QVTI_OK;
 }
 
-// Keep at most two chunks of the job's steps queued on its stream.
+// Keep at most two chunks of the job's steps queued on its stream.  Each
+// chunk ends with the non-finite sentinel; once a finished chunk reports a
+// NaN or Inf, no more steps are queued and the shot ends with
+// QVTI_ERR_NONFINITE (the other shots in flight are not affected).
 void qvti_server::top_up(Job* j)
 {
     while (j->enq < j->shot.nt) {
@@ -268,9 +278,14 @@ void qvti_server::top_up(Job* j)
             if (cudaEventQuery(j->chunk[0]) == cudaErrorNotReady) return;
             std::swap(j->chunk[0], j->chunk[1]);
             j->nchunk = 1;
+            if (*j->slot->nonfinite) {  // written in stream order before chunk[0]'s event
+                j->res.status = QVTI_ERR_NONFINITE;
+                j->enq = j->shot.nt;
+                break;
+            }
         }
         const int n = std::min(kChunk, j->shot.nt - j->enq);
-        if (qvti_step(j->slot->sim, n) != QVTI_OK) {
+        if (qvti_step(j->slot->sim, n) != QVTI_OK || qvti_check_finite_async(j->slot->sim, j->slot->nonfinite)) {
             j->res.status = qvti_last_error();
             j->enq = j->shot.nt;
             break;
@@ -291,6 +306,7 @@ void qvti_server::finish(Job* j, int status)
         if (e != cudaSuccess) status = QVTI_ERR_CUDA;
         float ms = 0.f;
         if (status == QVTI_OK && cudaEventElapsedTime(&ms, j->ev0, j->ev1) == cudaSuccess) j->res.device_ms = ms;
+        if (status == QVTI_OK && *j->slot->nonfinite) status = QVTI_ERR_NONFINITE;
         if (status == QVTI_OK)
             status = qvti_get_records(j->slot->sim, j->shot.rec_vx, j->shot.rec_vy, j->shot.rec_vz);
     }
@@ -509,7 +525,7 @@ extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_s
     const size_t ntp = (size_t)cfg->ntx * cfg->nty * cfg->ntz;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return QVTI_ERR_CUDA;
-    const size_t per = qvti_footprint_bytes(cfg->ntx, cfg->nty, cfg->ntz, cfg->vti);
+    const size_t per = qvti_footprint_bytes(cfg->ntx, cfg->nty, cfg->ntz, cfg->pml, cfg->vti);
     const int fit = (int)std::min<size_t>((size_t)max_active, std::max<size_t>(1, (size_t)(0.8 * free_b) / per));
     // homogeneous probe model (Vp 3000, Vs 1700, rho 2200, Qp 100, Qs 50)
     std::vector<float> vp(ntp, 3000.f), vs(ntp, 1700.f), rho(ntp, 2200.f);

@@ -525,11 +525,14 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                         // through the parameter struct the compiler cannot know)
                         const bool sx = in_slab(x, nx, pml), sy = in_slab(y, ny, pml), sz = in_slab(z, n, pml);
                         float qo[8], po[8];
+                        const int isx = sx ? slab_x(k, x, y, z) : 0, isy = sy ? slab_y(k, x, y, z) : 0,
+                                  isz = sz ? slab_z(k, x, y, z) : 0;
 #pragma unroll
                         for (int m = 0; m < 8; ++m) {
                             const bool on = m < 3 ? sx : (m < 6 ? sy : sz);
-                            qo[m] = on ? k.qn[m][ip] : 0.f;
-                            po[m] = on ? k.phn[m][ip] : 0.f;
+                            const int is = m < 3 ? isx : (m < 6 ? isy : isz);
+                            qo[m] = on ? k.qn[m][is] : 0.f;
+                            po[m] = on ? k.phn[m][is] : 0.f;
                         }
                         // loss: sum_terms tau-coefficient x (S - S_prev)/dt = (Q - Q_prev)/dt
                         const float Qxx = q11x + q12y + q13z, Qyy = q12x + q11y + q13z, Qzz = q13x + q13y + q33z;
@@ -557,7 +560,8 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
 #pragma unroll
                         for (int m = 0; m < 8; ++m) {
                             const bool on = m < 3 ? sx : (m < 6 ? sy : sz);
-                            if (on) { k.qn[m][ip] = qterm[m]; k.phn[m][ip] = ph[m]; }
+                            const int is = m < 3 ? isx : (m < 6 ? isy : isz);
+                            if (on) { k.qn[m][is] = qterm[m]; k.phn[m][is] = ph[m]; }
                         }
                     }
                     if (ip == src_ip && it < k.nt_rec) {  // cu:772-777, after the update
@@ -613,8 +617,11 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                         const int mA = (grp - 1) * 2, mB = mA + 1;
                         const bool onA = grp == 2 ? in_slab(y, ny, pml) : in_slab(z, n, pml);
                         const bool onB = grp == 3 ? in_slab(y, ny, pml) : in_slab(x, nx, pml);
-                        const float qoA = onA ? k.qs[mA][ip] : 0.f, poA = onA ? k.phs[mA][ip] : 0.f;
-                        const float qoB = onB ? k.qs[mB][ip] : 0.f, poB = onB ? k.phs[mB][ip] : 0.f;
+                        // A: z slab (xz, yz) or y slab (xy); B: x slab (xz, xy) or y slab (yz)
+                        const int isA = !onA ? 0 : grp == 2 ? slab_y(k, x, y, z) : slab_z(k, x, y, z);
+                        const int isB = !onB ? 0 : grp == 3 ? slab_y(k, x, y, z) : slab_x(k, x, y, z);
+                        const float qoA = onA ? k.qs[mA][isA] : 0.f, poA = onA ? k.phs[mA][isA] : 0.f;
+                        const float qoB = onB ? k.qs[mB][isB] : 0.f, poB = onB ? k.phs[mB][isB] : 0.f;
                         const float aA = grp == 2 ? ty[2 * P + p] : tz[2 * n + z];
                         const float bA = grp == 2 ? ty[3 * P + p] : tz[3 * n + z];
                         const float aB = grp == 3 ? ty[2 * P + p] : axhv, bB = grp == 3 ? ty[3 * P + p] : bxhv;
@@ -624,8 +631,8 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                         sig = sig + dt * (dA + phA + dB + phB + L);
                         qg[ip] = Qs;
                         sg[ip] = sig;
-                        if (onA) { k.qs[mA][ip] = qA; k.phs[mA][ip] = phA; }
-                        if (onB) { k.qs[mB][ip] = qB; k.phs[mB][ip] = phB; }
+                        if (onA) { k.qs[mA][isA] = qA; k.phs[mA][isA] = phA; }
+                        if (onB) { k.qs[mB][isB] = qB; k.phs[mB][isB] = phB; }
                     }
                     if (grp == 1) D[(1 * P + p) * np1 + z] = sig;
                     if (grp == 3) D[(2 * P + p) * np1 + z] = sig;
@@ -672,14 +679,15 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             float* __restrict__ ph = k.php[f == 0 ? 8 : f == 1 ? 2 : 5];  // pzz_z, pxz_z, pyz_z
             const int ip = cell(k, x, y, i);
             const bool slab = in_slab(i, n, pml) && i < n - 1 && x < nx - 1 && y < ny - 1;
-            const float old = slab ? ph[ip] : 0.f;
+            const int is = slab ? slab_z(k, x, y, i) : 0;
+            const float old = slab ? ph[is] : 0.f;
             const float part = D[(f * P + p) * np1 + i];
             float r = part;
             if (slab) {
                 const float a = f == 0 ? tz[2 * n + i] : tz[i];
                 const float b = f == 0 ? tz[3 * n + i] : tz[n + i];
                 const float nw = old + dt * (-a * old - b * part);
-                ph[ip] = nw;
+                ph[is] = nw;
                 r += nw;
             }
             k.R[rc][ip] = r;
@@ -745,7 +753,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         fft_any<N, 16, kThreads, kPencil, true>(k.py, tw, X1, Zf, P, 1, P, load_i, store_i);
         // kEpi cells per thread and trip: all their loads are in flight at once
         for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
-            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            int ipu[kEpi], iu[kEpi], pu[kEpi], isu[kEpi];
             bool ok[kEpi], slab[kEpi];
             float r0[kEpi], r1[kEpi], p1[kEpi], p4[kEpi];
 #pragma unroll
@@ -757,10 +765,11 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
+                isu[u] = slab[u] ? slab_y(k, x, iu[u], z) : 0;
                 r0[u] = ok[u] ? R0[ipu[u]] : 0.f;
                 r1[u] = ok[u] ? R1[ipu[u]] : 0.f;
-                p1[u] = slab[u] ? f1[ipu[u]] : 0.f;
-                p4[u] = slab[u] ? f4[ipu[u]] : 0.f;
+                p1[u] = slab[u] ? f1[isu[u]] : 0.f;
+                p4[u] = slab[u] ? f4[isu[u]] : 0.f;
             }
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
@@ -773,8 +782,8 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                     const float q4 = p4[u] + dt * (-k.ayh[i] * p4[u] - k.byh[i] * dy);
                     rx += q1;
                     ry += q4;
-                    f1[ip] = q1;
-                    f4[ip] = q4;
+                    f1[isu[u]] = q1;
+                    f4[isu[u]] = q4;
                 }
                 R0[ip] = rx;
                 R1[ip] = ry;
@@ -802,7 +811,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
         };
         fft_any<N, 8, kThreads, kPencil, true>(k.py, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
         for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
-            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            int ipu[kEpi], iu[kEpi], pu[kEpi], isu[kEpi];
             bool ok[kEpi], slab[kEpi];
             float r2[kEpi], p7[kEpi];
 #pragma unroll
@@ -814,8 +823,9 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                 const int z = z0 + pu[u];
                 ipu[u] = cell(k, x, iu[u], z);
                 slab[u] = ok[u] && in_slab(iu[u], ny, pml) && xin && iu[u] < ny - 1 && z < k.nz - 1;
+                isu[u] = slab[u] ? slab_y(k, x, iu[u], z) : 0;
                 r2[u] = ok[u] ? R2[ipu[u]] : 0.f;
-                p7[u] = slab[u] ? f7[ipu[u]] : 0.f;
+                p7[u] = slab[u] ? f7[isu[u]] : 0.f;
             }
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
@@ -826,7 +836,7 @@ __global__ void __launch_bounds__(kThreads) k_vy(KP k, int P_rt)
                 if (slab[u]) {
                     const float q7 = p7[u] + dt * (-k.ay[i] * p7[u] - k.by[i] * dz);
                     rz += q7;
-                    f7[ip] = q7;
+                    f7[isu[u]] = q7;
                 }
                 R2[ip] = rz;
             }
@@ -894,7 +904,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         };
         fft_any<N, 16, kThreads, kPencil, true>(k.px, tw, X1, Zf, P, 1, P, load_i, store_i);
         for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
-            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            int ipu[kEpi], iu[kEpi], pu[kEpi], isu[kEpi];
             bool ok[kEpi], slab[kEpi];
             float a0[kEpi], a1[kEpi], r0[kEpi], r1[kEpi], w0[kEpi], w1[kEpi], p0[kEpi], p3[kEpi];
 #pragma unroll
@@ -906,6 +916,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
                 ok[u] = t < n * P && iu[u] < nx - 1 && yin && z < k.nz - 1;
                 ipu[u] = cell(k, iu[u], y, z);
                 slab[u] = ok[u] && in_slab(iu[u], nx, pml);
+                isu[u] = slab[u] ? slab_x(k, iu[u], y, z) : 0;
                 const int ip = ipu[u];
                 a0[u] = ok[u] ? v0[ip] : 0.f;
                 a1[u] = ok[u] ? v1[ip] : 0.f;
@@ -913,8 +924,8 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
                 r1[u] = ok[u] ? R1[ip] : 0.f;
                 w0[u] = ok[u] ? ri0[ip] : 0.f;
                 w1[u] = ok[u] ? ri1[ip] : 0.f;
-                p0[u] = slab[u] ? f0[ip] : 0.f;
-                p3[u] = slab[u] ? f3[ip] : 0.f;
+                p0[u] = slab[u] ? f0[isu[u]] : 0.f;
+                p3[u] = slab[u] ? f3[isu[u]] : 0.f;
             }
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
@@ -926,8 +937,8 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
                     const float q3 = p3[u] + dt * (-k.ax[i] * p3[u] - k.bx[i] * py);
                     px += q0;
                     py += q3;
-                    f0[ip] = q0;
-                    f3[ip] = q3;
+                    f0[isu[u]] = q0;
+                    f3[isu[u]] = q3;
                 }
                 v0[ip] = a0[u] + dt * w0[u] * (px + r0[u]);
                 v1[ip] = a1[u] + dt * w1[u] * (py + r1[u]);
@@ -955,7 +966,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
         };
         fft_any<N, 8, kThreads, kPencil, true>(k.px, tw, X1, Zf, Qp, 1, Qp, load_i, store_i);
         for (int t0 = threadIdx.x; t0 < n * P; t0 += kEpi * blockDim.x) {
-            int ipu[kEpi], iu[kEpi], pu[kEpi];
+            int ipu[kEpi], iu[kEpi], pu[kEpi], isu[kEpi];
             bool ok[kEpi], slab[kEpi];
             float a2[kEpi], r2[kEpi], w2[kEpi], p6[kEpi];
 #pragma unroll
@@ -967,10 +978,11 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
                 ok[u] = t < n * P && iu[u] < nx - 1 && yin && z < k.nz - 1;
                 ipu[u] = cell(k, iu[u], y, z);
                 slab[u] = ok[u] && in_slab(iu[u], nx, pml);
+                isu[u] = slab[u] ? slab_x(k, iu[u], y, z) : 0;
                 a2[u] = ok[u] ? v2[ipu[u]] : 0.f;
                 r2[u] = ok[u] ? R2[ipu[u]] : 0.f;
                 w2[u] = ok[u] ? ri2[ipu[u]] : 0.f;
-                p6[u] = slab[u] ? f6[ipu[u]] : 0.f;
+                p6[u] = slab[u] ? f6[isu[u]] : 0.f;
             }
 #pragma unroll
             for (int u = 0; u < kEpi; ++u) {
@@ -980,7 +992,7 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
                 if (slab[u]) {
                     const float q6 = p6[u] + dt * (-k.ax[i] * p6[u] - k.bx[i] * pz);
                     pz += q6;
-                    f6[ip] = q6;
+                    f6[isu[u]] = q6;
                 }
                 v2[ip] = a2[u] + dt * w2[u] * (pz + r2[u]);
             }
@@ -1313,6 +1325,7 @@ int configure_kernels()
             set((const void*)k_mx<N>);
             set((const void*)k_sigma<N, false>);
             if constexpr (N > 0) set((const void*)k_sigma<N, true>);
+
             set((const void*)k_vy<N, false>);
             set((const void*)k_vx<N, false>);
             if constexpr (N > 0) {
@@ -1323,6 +1336,8 @@ int configure_kernels()
     set((const void*)k_deriv1d);
     set((const void*)kq_mx);
     set((const void*)kq_iz);
+    const int et = configure_tc_kernels();
+    if (et) e = (cudaError_t)et;
     return (int)e;
 }
 
@@ -1383,19 +1398,28 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         const int nb = kz0 + batch <= k.nkz ? batch : k.nkz - kz0;
         const long long line0 = (long long)kz0 * k.nx, line_end = line0 + (long long)nb * k.nx;
         const int ncy = cdiv(nb * k.nx, L);
-        dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, false><<<dim3(ncy, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L, line0,
-                                                                                                  line_end);
-        });
+        const bool tc = k.form == kFormTc && tc_cy_available(k);
+        if (tc) {
+            launch_cy_tc(k, false, 3, line0, line_end, st);
+        } else {
+            dispatch_len(len(k.ny, L, 8), [&](auto NN) {
+                k_cy<decltype(NN)::value, false><<<dim3(ncy, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L, line0,
+                                                                                                      line_end);
+            });
+        }
         mark(3);
         dispatch_len(len(k.nx, Pm, 16), [&](auto NN) {
             k_mx<decltype(NN)::value><<<dim3(cdiv(k.ny, Pm), nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
         });
         mark(4);
-        dispatch_len(len(k.ny, L, 8), [&](auto NN) {
-            k_cy<decltype(NN)::value, true><<<dim3(ncy, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L, line0,
-                                                                                                 line_end);
-        });
+        if (tc) {
+            launch_cy_tc(k, true, kNumGxy, line0, line_end, st);
+        } else {
+            dispatch_len(len(k.ny, L, 8), [&](auto NN) {
+                k_cy<decltype(NN)::value, true><<<dim3(ncy, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L, line0,
+                                                                                                     line_end);
+            });
+        }
         mark(5);
     }
     const int Ps = T.sigma;

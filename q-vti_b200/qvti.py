@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(HERE, "libqvti.so")
 
 SRC_FORCE_X = 0
 SRC_EXPLOSIVE = 1
+FORM_PLAIN = 0  # every transform stage as FP32 butterflies
+FORM_TC = 1     # 256-point y transforms as split-precision tensor-core contractions
 FIELDS = ("vx", "vy", "vz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz")
 
 
@@ -72,9 +74,11 @@ def lib():
             raise QvtiError("libqvti.so not found at %s: build it with `make -C q-vti_b200`" % LIB_PATH)
         L = ctypes.CDLL(LIB_PATH)
         sig = {
-            "qvti_footprint_bytes": (ctypes.c_size_t, [ctypes.c_int] * 4),
+            "qvti_footprint_bytes": (ctypes.c_size_t, [ctypes.c_int] * 5),
             "qvti_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(_V)]),
             "qvti_destroy": (ctypes.c_int, [_V]),
+            "qvti_get_config": (ctypes.c_int, [_V, ctypes.POINTER(Config)]),
+            "qvti_sims_created": (ctypes.c_longlong, []),
             "qvti_set_model": (ctypes.c_int, [_V, _F, _F, _F, _F, _F, _F, _F, ctypes.c_int]),
             "qvti_set_source": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F,
                                                ctypes.c_int]),
@@ -102,6 +106,7 @@ def lib():
             "qvti_profile_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _I, ctypes.c_char_p, _F, _D]),
             "qvti_get_stream": (ctypes.c_int, [_V, ctypes.POINTER(_V)]),
             "qvti_set_kz_batch": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_set_form": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_server_create": (ctypes.c_int, [ctypes.POINTER(SchedOpts), ctypes.POINTER(_V)]),
             "qvti_server_submit": (ctypes.c_int, [_V, ctypes.POINTER(Shot), ctypes.POINTER(ctypes.c_longlong)]),
             "qvti_server_wait": (ctypes.c_int, [_V, ctypes.c_longlong, ctypes.c_double,
@@ -138,8 +143,8 @@ def _f32(a, shape=None):
     return np.ascontiguousarray(a)
 
 
-def footprint_bytes(ntx, nty, ntz, vti=False):
-    return int(lib().qvti_footprint_bytes(ntx, nty, ntz, 1 if vti else 0))
+def footprint_bytes(ntx, nty, ntz, pml, vti=False):
+    return int(lib().qvti_footprint_bytes(ntx, nty, ntz, int(pml), 1 if vti else 0))
 
 
 class Simulation:
@@ -200,6 +205,10 @@ class Simulation:
         self.rn = rx.size
         _check(lib().qvti_set_receivers(self._h, int(r_iz), rx.ctypes.data_as(_I), ry.ctypes.data_as(_I), rx.size),
                "qvti_set_receivers")
+
+    def set_form(self, form):
+        """FORM_PLAIN or FORM_TC (qvti_set_form)."""
+        _check(lib().qvti_set_form(self._h, int(form)), "qvti_set_form")
 
     def reset(self):
         _check(lib().qvti_reset(self._h), "qvti_reset")
@@ -298,14 +307,18 @@ def simulation_for_case(c, vti=False, device=0):
                       vti=vti, device=device)
 
 
-def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=True, device=0, want_state=False):
+def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=True, device=0, want_state=False,
+             form=FORM_PLAIN):
     """Run a shot described by a case dict (tests/qvti_cases.py conventions).
 
     Returns dict(rec=[3, nt, rn], snaps={k: [3, ...]}, state=[9, ...] or None).
-    ``ref_offset`` adds the reference's +10 to s_iz (cuviscoelas_3D.cu:772)."""
+    ``ref_offset`` adds the reference's +10 to s_iz (cuviscoelas_3D.cu:772);
+    ``form`` selects the transforms' form (FORM_PLAIN, FORM_TC)."""
     nt = int(c["nt"] if nt is None else nt)
     snaps = sorted(int(s) for s in snaps)
     with simulation_for_case(c, vti=vti, device=device) as sim:
+        if form != FORM_PLAIN:
+            sim.set_form(form)
         sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"],
                       c.get("eps") if vti else None, c.get("delta") if vti else None)
         sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])

@@ -10,7 +10,10 @@ writes one compressed ``.npz`` per case into OUTDIR; the committed fixtures in
 tests/golden/ are exactly these files.  Each holds the case inputs (scalars,
 model arrays when heterogeneous, wavelet, receivers) and the reference's
 outputs: seismograms ``rec_vx/vy/vz`` ([it][ir], viscoelas_3D.cpp:416-435)
-and wavefield snapshots ``snap_<k>`` (vx, vy, vz after k steps).
+and wavefield snapshots ``snap_<k>`` (vx, vy, vz after k steps); for the
+96^3 configuration, whose full fields are too large to commit, the x-z plane
+12 cells beside the source ``plane_y_<k>`` (vx, vy, vz) every 100 steps and the
+per-field norms of the final state.  ``--only NAME`` regenerates one case.
 """
 import ctypes
 import os
@@ -69,7 +72,7 @@ def golden_cases():
     return [
         (qc.homogeneous_case(name="homog32"), [60, 120]),
         (qc.heterogeneous_case(name="hetero24x40x32"), [100]),
-        (qc.config1_case(nt=500), []),
+        (qc.config1_case(nt=500), [100, 200, 300, 400, 500]),
     ]
 
 
@@ -111,18 +114,29 @@ def save_case(outdir, c, snaps, lib=None):
                 continue
             _, f, _ = _run_isolated(c, k)
             out["snap_%d" % k] = f[:3].copy()
-    else:  # large case: keep per-field norms of the final state only
+    else:  # large case: per-field norms of the final state, x-z planes through the source
         out["final_norms"] = np.array([np.linalg.norm(f.astype(np.float64)) for f in fields])
+        py = int(c["s_iy"]) + 12  # off the source's plane: vy is antisymmetric about it
+        out["plane_y"] = np.array(py)
+        for k in snaps:
+            f = fields if k == c["nt"] else _run_isolated(c, k)[1]
+            out["plane_y_%d" % k] = f[:3, :, py, :].copy()
     path = os.path.join(outdir, c["name"] + ".npz")
     np.savez_compressed(path, **out)
     print("wrote", path, "ref %.1f ms" % ms, flush=True)
 
 
 def main():
-    outdir = sys.argv[1] if len(sys.argv) > 1 else "golden_out"
-    os.makedirs(outdir, exist_ok=True)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("outdir", nargs="?", default="golden_out")
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    os.makedirs(a.outdir, exist_ok=True)
     for c, snaps in golden_cases():
-        save_case(outdir, c, snaps)
+        if a.only and c["name"] != a.only:
+            continue
+        save_case(a.outdir, c, snaps)
 
 
 if __name__ == "__main__":

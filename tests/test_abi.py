@@ -86,3 +86,35 @@ def test_host_driver_builds(qvti):
     import subprocess
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "q-vti_b200"), "driver"])
     assert os.access(os.path.join(ROOT, "q-vti_b200", "qvti_driver"), os.X_OK)
+
+
+def test_per_device_once_logic(tmp_path):
+    """Kernel attributes are per device: the once-per-device helper the
+    engine and the allocation-free entry point use runs its set-up once for
+    each device ordinal, retries after a failure and rejects ordinals out of
+    range.  Plain C++, compiled and run here without a GPU."""
+    import subprocess
+    src = tmp_path / "t.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include "per_device.h"
+int main() {
+    qvti::PerDeviceOnce<4> once;
+    int calls[4] = {0, 0, 0, 0};
+    int fail_next = 1;
+    auto setup = [&](int d) { return [&, d] { ++calls[d]; if (d == 2 && fail_next) { fail_next = 0; return 7; } return 0; }; };
+    int r0 = once.run(0, setup(0)), r0b = once.run(0, setup(0));
+    int r1 = once.run(1, setup(1));
+    int r2 = once.run(2, setup(2)), r2b = once.run(2, setup(2)), r2c = once.run(2, setup(2));
+    int rbad = once.run(4, setup(0)), rneg = once.run(-1, setup(0));
+    std::printf("%d %d %d %d %d %d %d %d | %d %d %d %d | %d %d %d\n", r0, r0b, r1, r2, r2b, r2c, rbad, rneg,
+                calls[0], calls[1], calls[2], calls[3], (int)once.done(0), (int)once.done(2), (int)once.done(3));
+    return 0;
+}
+''')
+    exe = tmp_path / "t"
+    subprocess.check_call(["g++", "-std=c++17", "-I", os.path.join(ROOT, "q-vti_b200", "csrc"), str(src), "-o", str(exe),
+                           "-pthread"])
+    out = subprocess.check_output([str(exe)], text=True).strip()
+    # device 0 and 1 set up once; device 2 fails once, then succeeds once and is not run again
+    assert out == "0 0 0 7 0 0 -1 -1 | 1 1 2 0 | 1 1 0", out

@@ -102,7 +102,7 @@ def test_server_budget_admits_one_at_a_time(qvti, alone):
     """A budget that holds one 64^3 simulation: shots queue for memory, the
     pool frees idle simulations of other grids, results stay exact."""
     reqs = _requests(qvti)
-    budget = int(qvti.footprint_bytes(64, 64, 64, True) * 1.2)
+    budget = int(qvti.footprint_bytes(64, 64, 64, 8, True) * 1.2)
     with qvti.Server(max_active=4, mem_budget=budget) as srv:
         tickets = [srv.submit(r) for r in reqs]
         seen_active = 0
@@ -126,3 +126,28 @@ def test_server_rejects_a_shot_beyond_the_budget(qvti):
     with qvti.Server(max_active=1, mem_budget=1 << 20) as srv:
         with pytest.raises(qvti.QvtiError, match="allocation"):
             srv.submit(req)
+
+
+def test_nonfinite_shot_fails_alone_in_the_mix(qvti, alone):
+    """Shot-level failure detection, the fault made on the host: one shot's
+    model holds a NaN (an interior cell of its P velocity).  The scheduler's
+    sentinel (a non-finite check of the velocities after every chunk of
+    steps) ends that shot early with QVTI_ERR_NONFINITE; the shots beside it
+    finish with seismograms bit-identical to running alone.  The NaN shot
+    runs long (2000 steps) so an early stop is visible in its device time."""
+    reqs = _requests(qvti)[:3]
+    bad_case = dict(_cases()[0][0])
+    bad_case["velp"] = bad_case["velp"].copy()
+    bad_case["velp"][16, 16, 12] = np.nan
+    bad_case["nt"] = 2000
+    bad_case["rik"] = qc.ricker(2000, bad_case["dt"], bad_case["f0"])
+    bad = qvti.ShotRequest(bad_case)
+    with qvti.Server(max_active=4) as srv:
+        tickets = [srv.submit(r) for r in (reqs[0], bad, reqs[1], reqs[2])]
+        res = [srv.wait(t) for t in tickets]
+    assert res[1]["status"] == 6, res[1]  # QVTI_ERR_NONFINITE
+    for r, req, ref in zip((res[0], res[2], res[3]), reqs, alone[:3]):
+        assert r["status"] == 0
+        assert np.array_equal(req.rec, ref)
+    # stopped after at most a few 32-step chunks of 2000
+    assert res[1]["latency_s"] < 20.0

@@ -67,10 +67,14 @@ def test_snapshot_size_and_header(qvti):
     with _prepared(qvti, c, True) as sim:
         sim.step(5)
         snap = sim.save_state()
-    ntp = 48 * 32 * 40
+    nx, ny, nz, pml = 48, 32, 40, int(c["pml"])
+    ntp = nx * ny * nz
     rn = int(c["rnx_max"] * c["rny_max"])
-    assert snap.size == 72 + 55 * 4 * ntp + 3 * 5 * rn * 4
-    assert bytes(snap[:8]) == b"QVTIST01"
+    # 18 full-grid arrays (v, s, R, Q) and the 37 C-PML arrays of their slabs:
+    # 13 of the x slab, 13 of the y slab, 11 of the z slab
+    slab = 13 * 2 * pml * ny * nz + 13 * nx * 2 * pml * nz + 11 * nx * ny * 2 * pml
+    assert snap.size == 72 + 18 * 4 * ntp + 4 * slab + 3 * 5 * rn * 4
+    assert bytes(snap[:8]) == b"QVTIST02"
 
 
 def test_mismatched_snapshots_are_rejected(qvti):

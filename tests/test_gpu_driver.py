@@ -9,6 +9,7 @@ shot run through the Python binding of the extended ABI (bit for bit: same
 kernels, same inputs).  The JSON-lines run log has one line per shot; a
 stepped run adds the energy norms, which equal the binding's.
 """
+import ctypes
 import json
 import os
 import subprocess
@@ -95,3 +96,62 @@ def test_driver_snapshots_match_fields(qvti, tmp_path):
     state = qvti.run_case(c, want_state=True)["state"].astype(np.float64)
     want = (state.reshape(9, -1) ** 2).sum(axis=1)
     assert np.allclose(entry["energy"], want, rtol=1e-9, atol=0)
+
+
+class _Source(ctypes.Structure):
+    _fields_ = [("s_iz", ctypes.c_int), ("s_ix", ctypes.c_int), ("s_iy", ctypes.c_int), ("r_iz", ctypes.c_int),
+                ("r_ix", ctypes.POINTER(ctypes.c_int)), ("r_iy", ctypes.POINTER(ctypes.c_int)), ("r_n", ctypes.c_int)]
+
+
+class _MultiGPU(ctypes.Structure):
+    _fields_ = [("record", ctypes.POINTER(ctypes.c_float)), ("record2", ctypes.POINTER(ctypes.c_float)),
+                ("record3", ctypes.POINTER(ctypes.c_float)), ("sim", ctypes.c_void_p),
+                ("ntx", ctypes.c_int), ("nty", ctypes.c_int), ("ntz", ctypes.c_int), ("nt", ctypes.c_int),
+                ("rnmax", ctypes.c_int)]
+
+
+def test_void_abi_keeps_its_engine_across_shots(qvti):
+    """The reference allocates once (cuda_Device_malloc) and runs every shot
+    on the same buffers (viscoelas_3D.cpp:355-405).  Three shots through
+    cuda_forward_acoustic_3D: the second (same grid and constants, another
+    source position) reuses the first shot's engine -- no qvti_create -- and
+    both equal qvti_forward_shot bit for bit; the third changes dt and gets a
+    new engine."""
+    L = qvti.lib()
+    F = ctypes.POINTER(ctypes.c_float)
+    L.qvti_sims_created.restype = ctypes.c_longlong
+    L.cuda_forward_acoustic_3D.restype = None
+    L.cuda_forward_acoustic_3D.argtypes = [ctypes.c_int] * 11 + [ctypes.c_float] * 7 + [F] * 6 + \
+        [ctypes.POINTER(_Source), ctypes.POINTER(_MultiGPU)] + [ctypes.c_int] * 5
+    c = qc.heterogeneous_case(n=(32, 32, 32), pml=6, nt=60, seed=9, src=(16, 16, 16), r_iz=8)
+    ntx, nty, ntz, nt = c["ntx"], c["nty"], c["ntz"], c["nt"]
+    ntp = ntx * nty * ntz
+    rnx, rny = int(c["rnx_max"]), int(c["rny_max"])
+    rn = rnx * rny
+    rix, riy = np.ascontiguousarray(c["r_ix"], np.int32), np.ascontiguousarray(c["r_iy"], np.int32)
+    IP = ctypes.POINTER(ctypes.c_int)
+    srcs = (_Source * 3)(*[_Source(int(c["s_iz"]), sx, 16, int(c["r_iz"]), rix.ctypes.data_as(IP),
+                                   riy.ctypes.data_as(IP), rn) for sx in (16, 13, 19)])
+    plan = (_MultiGPU * 1)()
+    L.cuda_Device_malloc(ntx, nty, ntz, ntp, ntx - 12, nty - 12, ntz - 12, nt, rn, plan, 1)
+    L.cuda_Host_initialization(ntp, nt, rn, plan, 1)
+    model = [np.ascontiguousarray(c[k], np.float32) for k in ("velp", "gama_p", "vels", "gama_s", "rho")]
+    rik = np.ascontiguousarray(c["rik"], np.float32)
+    w0 = float(np.float32(2 * qc.PI_REF * c["f0"]))
+    try:
+        created = []
+        for shot, dt in ((0, c["dt"]), (1, c["dt"]), (2, 0.5 * c["dt"])):
+            L.cuda_forward_acoustic_3D(0, shot, nt, ntx, nty, ntz, ntp, ntx - 12, nty - 12, ntz - 12, c["pml"],
+                                       c["dx"], c["dy"], c["dz"], dt, c["f0"], w0, 5000.0, rik.ctypes.data_as(F),
+                                       *[m.ctypes.data_as(F) for m in model], srcs, plan, 1, rn, rnx, rny, 4)
+            created.append(L.qvti_sims_created())
+            got = np.stack([np.ctypeslib.as_array(getattr(plan[0], r), shape=(nt, rn)).copy()
+                            for r in ("record", "record2", "record3")])
+            want = qvti.run_case(dict(c, s_ix=srcs[shot].s_ix, dt=dt))["rec"]
+            assert np.array_equal(got, want), "shot %d differs from qvti_forward_shot" % shot
+            assert np.abs(got).max() > 0
+        # run_case creates one simulation per call; the void ABI one on shot 0 and one on shot 2
+        assert created[1] - created[0] == 1, created   # only run_case's own simulation
+        assert created[2] - created[1] == 2, created   # a new engine for the new dt, plus run_case's
+    finally:
+        L.cuda_Device_free(plan, 1)

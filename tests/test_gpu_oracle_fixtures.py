@@ -1,0 +1,77 @@
+"""Parity on the benchmark model and on the small configuration as specified,
+against FP64 oracle fixtures (tests/golden/oracle/, made by
+tests/golden/make_oracle_golden.py; the oracle itself is pinned to the
+reference's cuFFT build in tests/test_oracle.py).
+
+* vti_crop128: the centred 128^3 crop of the 256^3 VTI benchmark model at the
+  benchmark's dt, 400 steps (the 128-point compiled kernels, a 20-cell
+  C-PML, strong heterogeneity and anisotropy over a long run).
+* config1_explosive: 96^3 isotropic, explosive source at the centre, 500
+  steps.
+
+Tolerance: relative L2 <= 1e-4 on every seismogram component and on the vx,
+vy, vz planes of every snapshot (every 100 steps).
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import qvti_cases as qc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = os.path.join(HERE, "golden", "oracle")
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_oracle_golden as mog  # noqa: E402
+
+TOL = 1e-4
+
+
+def _fixture(name):
+    path = os.path.join(FIX, name + ".npz")
+    if not os.path.exists(path):
+        pytest.fail("missing fixture %s (tests/golden/make_oracle_golden.py)" % path)
+    return dict(np.load(path))
+
+
+def _case(name):
+    c = mog.cases()[name]()
+    g = _fixture(name)
+    sums = mog.model_sums(c)
+    assert np.allclose(sums, g["model_sums"], rtol=1e-6, atol=0), "rebuilt model differs from the fixture's"
+    return c, g
+
+
+@pytest.mark.parametrize("name", sorted(mog.cases()))
+def test_fixture_cases_rebuild_their_models(name):
+    """CPU: the seeded generators rebuild the fixture's model and geometry."""
+    c, g = _case(name)
+    assert int(g["nt"]) == int(c["nt"]) and float(g["dt"]) == pytest.approx(float(c["dt"]))
+    assert np.array_equal(g["r_ix"], c["r_ix"]) and np.array_equal(g["r_iy"], c["r_iy"])
+    assert g["rec_vx"].shape == (int(c["nt"]), len(c["r_ix"]))
+    assert np.isfinite(g["rec_vx"]).all() and np.abs(g["rec_vx"]).max() > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(mog.cases()))
+def test_against_oracle_fixture(qvti, name):
+    c, g = _case(name)
+    nt = int(c["nt"])
+    snaps = list(range(100, nt + 1, 100))
+    ours = qvti.run_case(c, snaps=snaps, src_type=int(c["src_type"]), vti=bool(c["vti"]), ref_offset=False)
+    worst = 0.0
+    for i, comp in enumerate(("vx", "vy", "vz")):
+        e = qc.relL2(ours["rec"][i], g["rec_" + comp])
+        worst = max(worst, e)
+        assert e <= TOL, "%s seismogram %s relL2 %.3g" % (name, comp, e)
+    py, pz = int(c["plane_y"]), int(c["plane_z"])
+    for k in snaps:
+        f = ours["snaps"][k]
+        for i in range(3):
+            for lab, mine, ref in (("y", f[i][:, py, :], g["plane_y_%d" % k][i]),
+                                   ("z", f[i][:, :, pz], g["plane_z_%d" % k][i])):
+                e = qc.relL2(mine, ref)
+                worst = max(worst, e)
+                assert e <= TOL, "%s step %d field %d plane %s relL2 %.3g" % (name, k, i, lab, e)
+    print("%s worst relL2 %.2e" % (name, worst))

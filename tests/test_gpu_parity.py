@@ -43,11 +43,19 @@ def test_against_reference_golden(qvti, name):
 
 
 def test_config1_against_reference_golden(qvti):
-    """96^3, 20-cell C-PML, 500 steps: seismograms and final-state norms."""
+    """96^3, 20-cell C-PML, 500 steps: seismograms, the x-z plane through the
+    source of vx, vy, vz every 100 steps, and the final-state norms."""
     c = load_golden("config1")
-    ours = qvti.run_case(c, want_state=True)
+    planes = sorted(int(k.split("_")[2]) for k in c if k.startswith("plane_y_"))
+    assert planes == [100, 200, 300, 400, 500], planes
+    ours = qvti.run_case(c, snaps=planes, want_state=True)
     ref = dict(rec=np.stack([c["rec_vx"], c["rec_vy"], c["rec_vz"]]))
     _compare(ours, ref, "config1")
+    py = int(c["plane_y"])
+    for k in planes:
+        for i in range(3):
+            e = qc.relL2(ours["snaps"][k][i][:, py, :], c["plane_y_%d" % k][i])
+            assert e <= TOL, "config1 step %d field %d plane relL2 %.3g" % (k, i, e)
     norms = np.array([np.linalg.norm(f.astype(np.float64)) for f in ours["state"]])
     rel = np.abs(norms - c["final_norms"]) / c["final_norms"]
     assert rel.max() <= TOL, rel
@@ -116,6 +124,21 @@ def test_compile_time_path_against_oracle(qvti, oracle, n):
     _compare(ours, ref, "ct%dx%dx%d" % n)
 
 
+@pytest.mark.parametrize("n", [(256, 16, 24), (16, 256, 24), (24, 16, 256)])
+def test_256_point_kernels_against_oracle(qvti, oracle, n):
+    """The benchmark grid is 256 points on every axis; each case puts one axis
+    at 256 so the instantiations the benchmark times run against the FP64
+    oracle: x = 256 -> k_vx<256> and k_mx<256> (k-space x pass); y = 256 ->
+    k_vy<256> and both k_cy<256> passes; z = 256 -> k_fz<256> and
+    k_sigma<256> (its in-place two-stage C2R).  VTI, heterogeneous, 120
+    steps, seismograms and snapshots at steps 60 and 120."""
+    nt = 120
+    c = _ct_case(n, nt, pml=4)
+    ours = qvti.run_case(c, snaps=[60, nt], vti=True)
+    ref = oracle.run_case(c, snaps=[60, nt], vti=True)
+    _compare(ours, ref, "256axis%dx%dx%d" % n)
+
+
 @pytest.mark.parametrize("batch", [7, 17])
 def test_kz_batches_match_one_pass(qvti, batch):
     """The k-space passes in batches of kz planes (ragged line tiles at every
@@ -135,8 +158,8 @@ def test_kz_batches_match_one_pass(qvti, batch):
         assert np.array_equal(sim.fields(0, 9), full["state"])
 
 
-def _ct_case(n, nt):
-    c = qc.heterogeneous_case(n=n, pml=8, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=nt, f0=30.0, seed=21,
+def _ct_case(n, nt, pml=8):
+    c = qc.heterogeneous_case(n=n, pml=pml, d=(10.0, 10.0, 10.0), dt=0.8e-3, nt=nt, f0=30.0, seed=21,
                               src=(n[0] // 2, n[1] // 2, n[2] // 2), r_iz=n[2] // 2 - 6, name="ct")
     # a 3 x 3 receiver patch beside the source: the direct wave reaches every
     # receiver within the run, so the seismograms carry signal, not noise

@@ -53,3 +53,29 @@ def test_noalloc_rejects_grids_beyond_its_scratch(qvti):
     d = torch.empty(16, dtype=torch.float32, device="cuda")   # never touched: rejected first
     with pytest.raises(qvti.QvtiError, match="unsupported"):
         qvti.q_derivative_noalloc(d.data_ptr(), d.data_ptr(), (128, 128, 128), (10.0, 10.0, 10.0), 0, True, 0)
+    assert qvti.lib().qvti_last_error() == 3  # QVTI_ERR_UNSUPPORTED, reported like every other entry point
+    with pytest.raises(qvti.QvtiError, match="invalid argument"):
+        qvti.q_derivative_noalloc(d.data_ptr(), d.data_ptr(), (32, 32, 32), (10.0, 10.0, 10.0), 3, True, 0)
+    assert qvti.lib().qvti_last_error() == 1  # QVTI_ERR_ARG
+
+
+def test_noalloc_matches_fp64_numpy(qvti, oracle):
+    """The allocation-free derivative against an FP64 numpy restatement of
+    the operator itself (tests/test_gpu_derivative.py: Re IFFT3(|k|^p T(k_a)
+    FFT3(f)) with the oracle's k-space tables), not only against the
+    allocating entry point."""
+    import torch
+    from test_gpu_derivative import _numpy_q_derivative
+
+    shape, spacing = (32, 48, 40), (10.0, 8.0, 12.0)
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal(shape).astype(np.float32)
+    d_in = torch.from_numpy(f).cuda()
+    d_out = torch.empty_like(d_in)
+    for axis, fw, pw in ((1, True, 1), (0, False, -1), (2, True, 0)):
+        d_out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        qvti.q_derivative_noalloc(d_in.data_ptr(), d_out.data_ptr(), shape, spacing, axis, fw, pw, stream=0)
+        torch.cuda.synchronize()
+        want = _numpy_q_derivative(f, spacing, axis, fw, pw, oracle)
+        assert _rel(d_out.cpu().numpy(), want) <= TOL
