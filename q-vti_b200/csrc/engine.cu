@@ -414,6 +414,7 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.err = s->d_err;
     k.form = kFormPlain;
 
+
     for (int j = 0; j < 5; ++j) k.MU[j] = mu[j];
     k.mrho = s->coef[0]; k.mgp = s->coef[1]; k.mgs = s->coef[2];
     k.mc33 = s->coef[4]; k.mcs = s->coef[6];

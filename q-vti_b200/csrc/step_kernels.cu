@@ -276,37 +276,55 @@ constexpr int kSigmaRows = 4;  // y rows per k_sigma tile (compile-time path)
 // (37 KB at 256 points, so three blocks fit an SM instead of two).
 constexpr bool sigma_inplace(int n) { return n > 0; }
 constexpr int sigma_threads(int n) { return sigma_inplace(n) ? 9 * kSigmaRows / 2 * 16 : kThreads; }
-constexpr size_t sigma_smem_ct(int n)  // smem_sigma for a compile-time length
+// Compile-time lengths can run the 27 fields as three groups of nine
+// (normal; xz and the A half of xy; the B half of xy and yz), every transform
+// stage a full round of 288 butterflies; the xy update's A half is folded into
+// the stored sxy and Qxy in the first shear group and completed in the next.
+constexpr bool sigma_regroup(int n) { return n > 0; }
+// Two-stage compile-time lengths can keep the z-derivative pass's stresses
+// out of a buffer of their own: the pass re-reads the stresses the update
+// has just stored (L2) and parks its results in the transform buffer, which
+// is free by then.  The smaller tile leaves the SM more L1.
+constexpr bool sigma_nod_ok(int n) { return n > 0 && ct_nst(n) == 2; }
+constexpr size_t sigma_smem_ct(int n, bool nod = false)  // smem_sigma for a compile-time length
 {
     const size_t bufA = (size_t)9 * (kSigmaRows / 2) * (n + n / 16);  // float2
     const size_t nb = ct_nst(n) > 2 ? 2 : 1;
     const size_t sreal = sigma_inplace(n) ? 0 : (size_t)9 * kSigmaRows * (n + 1);
-    return 8 * ((size_t)n + nb * bufA + 2 * (size_t)n) +
-           4 * (sreal + (size_t)3 * kSigmaRows * (n + 1) + 4 * (size_t)n + 4 * kSigmaRows);
+    const size_t dbuf = nod ? 0 : (size_t)3 * kSigmaRows * (n + 1);
+    return 8 * ((size_t)n + nb * bufA + 2 * (size_t)n) + 4 * (sreal + dbuf + 4 * (size_t)n + 4 * kSigmaRows);
 }
 // Resident blocks per SM the register budget is sized for: as many as the
 // tile's shared memory admits (at most 3), so a length whose tiles already
 // limit residency gets the registers to keep more loads in flight.
-constexpr int sigma_min_blocks(int n)
+constexpr int sigma_min_blocks(int n, bool nod = false)
 {
     if (n == 0) return 3;
-    const size_t b = (228 * 1024) / (sigma_smem_ct(n) + 1024);
+    const size_t b = (228 * 1024) / (sigma_smem_ct(n, nod) + 1024);
     return b < 1 ? 1 : b > 3 ? 3 : (int)b;
 }
 constexpr int sigma_cells(int n) { return (n == 256 && !sigma_inplace(n)) ? 2 : 1; }
 
 // z-pencils of one x and P y rows (P/2 pencil pairs): C2R of the 27
-// derivative fields group by group (normal: G 0..8, xz: 9..14, xy: 15..20,
-// yz: 21..26), each group batched into one transform and followed by its
-// stress update; then the z derivatives of the new szz, sxz, syz for the next
-// velocity update (cu:1279-1306: partz2, partz1, partz3) with their C-PML
-// z terms, and the source injection.
+// derivative fields group by group, each group batched into one transform
+// and followed by its stress update; then the z derivatives of the new szz,
+// sxz, syz for the next velocity update (cu:1279-1306: partz2, partz1,
+// partz3) with their C-PML z terms, and the source injection.  Groups on the
+// compile-time path: normal (G 0..8), xz with the A half of xy (9..17), the
+// B half of xy with yz (18..26) -- nine fields, 288 butterflies per stage,
+// one per thread; on the runtime path: normal, xz, xy, yz (9, 6, 6, 6).  At
+// two-stage lengths the z pass re-reads the stresses it differentiates
+// (just stored, in L2) instead of buffering them: the 12 KB saved lets the
+// SM keep ~92 KB of L1 beside three resident tiles (measured at 256^3:
+// 2.14 ms with four groups and the buffer, 2.08 with either change, 1.95
+// with both).
 //
 // RAG: the grid's last y tile is partial (ny not a multiple of the tile); a
 // separate instantiation, so the masks cost the full tiles no registers.
 template <int N, bool RAG>
-__global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma(KP k, int P_rt)
+__global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_nod_ok(N))) k_sigma(KP k, int P_rt)
 {
+    constexpr bool REGRP = sigma_regroup(N), NOD = sigma_nod_ok(N);
     constexpr bool INPLACE = sigma_inplace(N);
     constexpr int NT = sigma_threads(N);
     extern __shared__ float4 smem4[];
@@ -325,10 +343,14 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     // place, the group's real fields live there
     float2* Lb = (N > 0 && ((ct_nst(N) - 2) & 1)) ? B : A;
     float* S = reinterpret_cast<float*>(B + (two_buf ? bufA : 0));  // not used in place
-    float* D = INPLACE ? S : S + 9 * P * np1;                         // [3][P][np1]: szz sxz syz
-    float* tz = D + 3 * P * np1;                                          // [4][n]: az bz azh bzh
+    // [3][P][np1]: szz sxz syz for the z pass (NOD: in the transform buffer
+    // past the z pass's own stage buffer of 6 line-padded pencils, used only
+    // once the groups are done)
+    float* D = NOD ? reinterpret_cast<float*>(A + 3 * (kSigmaRows / 2) * (n + n / 16)) : INPLACE ? S : S + 9 * P * np1;
+    float* tz = NOD ? reinterpret_cast<float*>(A + bufA) : D + 3 * P * np1;  // [4][n]: az bz azh bzh
     float* ty = tz + 4 * n;                                               // [4][P]: ay by ayh byh of the rows
     float2* tzs = reinterpret_cast<float2*>(ty + 4 * P);                  // [2][n]: Fz Bz
+    constexpr int NGRP = REGRP ? 3 : 4;
     const int x = blockIdx.y, y0 = blockIdx.x * P;
     const int yv = RAG ? min(P, ny - y0) : P;  // rows of the tile inside the grid (even)
     load_table(tw, k.tw_z, n);
@@ -370,7 +392,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
     // first stage, which keeps 16 loads per thread in flight; prefetching
     // them 32 bytes at a time cost more instructions than it saved.)
     auto prefetch_group = [&](int g) {
-        if (g > 3) return;
+        if (g >= NGRP) return;
         const int c0 = cell(k, x, y0, 0);
         const unsigned run = 4u * yv * n;
         if (threadIdx.x == 0) {
@@ -379,18 +401,53 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                                         k.mc11, k.mc33, k.mc13, k.mcs};
                 for (int a = 0; a < 13; ++a) prefetch_l2(arr[a] + c0, run);
             } else {
-                const int sidx = g == 1 ? 4 : g == 2 ? 3 : 5;
-                prefetch_l2(k.s[sidx] + c0, run);
-                prefetch_l2(k.Q[sidx] + c0, run);
+                // stresses and loss potentials the group updates (REGRP: xz;
+                // xy and yz), then the shear set
+                const int s1 = REGRP ? (g == 1 ? 4 : 3) : (g == 1 ? 4 : g == 2 ? 3 : 5);
+                prefetch_l2(k.s[s1] + c0, run);
+                prefetch_l2(k.Q[s1] + c0, run);
+                if (REGRP && g == 2) {
+                    prefetch_l2(k.s[5] + c0, run);
+                    prefetch_l2(k.Q[5] + c0, run);
+                }
                 for (int j = 0; j < 5; ++j) prefetch_l2(k.MU[j] + c0, run);
             }
         }
     };
     prefetch_group(0);
 
-    for (int grp = 0; grp < 4; ++grp) {
-        const int NF = grp == 0 ? 9 : 6;
-        const int o0 = grp == 0 ? 0 : 9 + (grp - 1) * 6;
+    // C-PML state of one shear term: g the shear component (1 xz, 2 xy, 3
+    // yz), hb its B half (xz vz_x, xy vy_x, yz vz_y) or A half (xz vx_z,
+    // xy vx_y, yz vy_z); the slab it lives in, its memory variables (loaded
+    // here) and profile.
+    struct ShearTerm {
+        bool on;
+        int is, m;
+        float qo, po, a, b;
+    };
+    auto shear_term = [&](int g, bool hb, int p, int y, int z) -> ShearTerm {
+        ShearTerm t;
+        t.m = (g - 1) * 2 + (hb ? 1 : 0);
+        const bool ysl = hb ? g == 3 : g == 2;  // y slab; otherwise A: z slab, B: x slab
+        t.on = ysl ? in_slab(y, ny, pml) : hb ? in_slab(x, nx, pml) : in_slab(z, n, pml);
+        t.is = !t.on ? 0 : ysl ? slab_y(k, x, y, z) : hb ? slab_x(k, x, y, z) : slab_z(k, x, y, z);
+        t.qo = t.on ? k.qs[t.m][t.is] : 0.f;
+        t.po = t.on ? k.phs[t.m][t.is] : 0.f;
+        t.a = ysl ? ty[2 * P + p] : hb ? axhv : tz[2 * n + z];
+        t.b = ysl ? ty[3 * P + p] : hb ? bxhv : tz[3 * n + z];
+        return t;
+    };
+    auto shear_ph = [&](const ShearTerm& t, float d, float q) {
+        const float T = d + (q - t.qo) * inv_dt;
+        return t.on ? t.po + dt * (-t.a * t.po - t.b * T) : 0.f;
+    };
+    auto shear_store = [&](const ShearTerm& t, float q, float ph) {
+        if (t.on) { k.qs[t.m][t.is] = q; k.phs[t.m][t.is] = ph; }
+    };
+
+    for (int grp = 0; grp < NGRP; ++grp) {
+        const int NF = (REGRP || grp == 0) ? 9 : 6;
+        const int o0 = REGRP ? 9 * grp : grp == 0 ? 0 : 9 + (grp - 1) * 6;
         const int npen = NF * Qp;
         prefetch_group(grp + 1);
         // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
@@ -430,7 +487,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
             // which keeps the 256-point transform free of register spill;
             // multi-round stages stay loops (ROLL) for the same reason at the
             // lengths with small radices.
-            if (grp == 0) {
+            if (REGRP || grp == 0) {
                 using F = FftCT<N, 9 * kSigmaRows / 2, NT, kPencil, ct_nst(N) == 2, true>;
                 auto keep = [&](int pp, int i, float2 v) { Lb[F::at(pp, i)] = v; };
                 F::template run<true>(tw, A, B, load, keep);
@@ -449,8 +506,8 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         auto sval = [&](int f, int p, int z) -> float {
             if constexpr (INPLACE) {
                 const int pp = f * Qp + (p >> 1);
-                const int slot = grp == 0 ? FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>::at(pp, z)
-                                          : FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>::at(pp, z);
+                const int slot = (REGRP || grp == 0) ? FftCT<N, 9 * kSigmaRows / 2, NT, kPencil>::at(pp, z)
+                                                     : FftCT<N, 6 * kSigmaRows / 2, NT, kPencil>::at(pp, z);
                 return Af[2 * slot + (p & 1)];
             } else {
                 return S[(f * P + p) * np1 + z];
@@ -461,6 +518,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         //    are in flight together (the arrays cannot alias, but the
         //    compiler cannot know that through the parameter struct).
         constexpr int kCells = sigma_cells(N);
+        static_assert(!REGRP || kCells == 1, "the regrouped updates take one cell per trip");
         for (int t0 = threadIdx.x; t0 < P * n; t0 += kCells * blockDim.x) {
             if (grp == 0) {
                 float* __restrict__ s0 = k.s[0];
@@ -573,9 +631,9 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                         }
                     }
                     if (upd || ip == src_ip) { s0[ip] = sxx; s1[ip] = syy; s2[ip] = szz; }
-                    D[(0 * P + p) * np1 + z] = szz;
+                    if constexpr (!NOD) D[(0 * P + p) * np1 + z] = szz;
                 }
-            } else {
+            } else if (!REGRP) {
                 const int sidx = grp == 1 ? 4 : grp == 2 ? 3 : 5;  // sxz, sxy, syz in s[]
                 float* __restrict__ sg = k.s[sidx];
                 float* __restrict__ qg = k.Q[sidx];
@@ -634,8 +692,94 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
                         if (onA) { k.qs[mA][isA] = qA; k.phs[mA][isA] = phA; }
                         if (onB) { k.qs[mB][isB] = qB; k.phs[mB][isB] = phB; }
                     }
-                    if (grp == 1) D[(1 * P + p) * np1 + z] = sig;
-                    if (grp == 3) D[(2 * P + p) * np1 + z] = sig;
+                    if constexpr (!NOD) {
+                        if (grp == 1) D[(1 * P + p) * np1 + z] = sig;
+                        if (grp == 3) D[(2 * P + p) * np1 + z] = sig;
+                    }
+                }
+            } else if (grp == 1) {
+                // xz, and the A half (dy vx: y slab) of xy: with
+                // dt L = Qxy - Qxy_old, sxy_new = sxy + dt (dA + phA) + qA - Qxy_old
+                // + dt (dB + phB) + qB and Qxy_new = qA + qB; the A part goes
+                // into the stored sxy and Qxy now, the B part in the next group
+                float* __restrict__ sg = k.s[4];
+                float* __restrict__ qg = k.Q[4];
+                float* __restrict__ sxy = k.s[3];
+                float* __restrict__ qxy = k.Q[3];
+                {
+                    const int t = t0;  // one cell per thread and trip (kCells == 1)
+                    if (RAG && t / n >= yv) continue;
+                    const int p = t / n, z = t - p * n, y = y0 + p;
+                    const int ip = cell(k, x, y0 + p, z);
+                    const float s_old = sg[ip], q_old = qg[ip], sxy_old = sxy[ip], qxy_old = qxy[ip];
+                    float mu[5];
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) mu[j] = __ldg(k.MU[j] + ip);
+                    const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
+                    auto sv = [&](int f) { return sval(f, p, z); };
+                    float sig = s_old;
+                    if (upd) {
+                        const float A0 = sv(0), A1 = sv(1), A2 = sv(2), B0 = sv(3), B1 = sv(4), B2 = sv(5);
+                        const float C0 = sv(6), C1 = sv(7), C2 = sv(8);
+                        const float dA = mu[0] * A0 + mu[1] * A1 + mu[2] * A2, qA = mu[3] * A0 + mu[4] * A1;
+                        const float dB = mu[0] * B0 + mu[1] * B1 + mu[2] * B2, qB = mu[3] * B0 + mu[4] * B1;
+                        const float dC = mu[0] * C0 + mu[1] * C1 + mu[2] * C2, qC = mu[3] * C0 + mu[4] * C1;
+                        const float Qs = qA + qB;
+                        const float L = (Qs - q_old) * inv_dt;
+                        const ShearTerm tA = shear_term(1, false, p, y, z), tB = shear_term(1, true, p, y, z);
+                        const ShearTerm tC = shear_term(2, false, p, y, z);
+                        const float phA = shear_ph(tA, dA, qA), phB = shear_ph(tB, dB, qB), phC = shear_ph(tC, dC, qC);
+                        sig = sig + dt * (dA + phA + dB + phB + L);
+                        qg[ip] = Qs;
+                        sg[ip] = sig;
+                        shear_store(tA, qA, phA);
+                        shear_store(tB, qB, phB);
+                        shear_store(tC, qC, phC);
+                        sxy[ip] = sxy_old + dt * (dC + phC) + (qC - qxy_old);
+                        qxy[ip] = qC;
+                    }
+                    if constexpr (!NOD) D[(1 * P + p) * np1 + z] = sig;
+                }
+            } else {
+                // the B half (dx vy: x slab) of xy, then yz
+                float* __restrict__ sxy = k.s[3];
+                float* __restrict__ qxy = k.Q[3];
+                float* __restrict__ syz = k.s[5];
+                float* __restrict__ qyz = k.Q[5];
+                {
+                    const int t = t0;  // one cell per thread and trip (kCells == 1)
+                    if (RAG && t / n >= yv) continue;
+                    const int p = t / n, z = t - p * n, y = y0 + p;
+                    const int ip = cell(k, x, y0 + p, z);
+                    const float sxy_a = sxy[ip], qxy_a = qxy[ip], syz_old = syz[ip], qyz_old = qyz[ip];
+                    float mu[5];
+#pragma unroll
+                    for (int j = 0; j < 5; ++j) mu[j] = __ldg(k.MU[j] + ip);
+                    const bool upd = x < nx - 1 && y < ny - 1 && z < n - 1;
+                    auto sv = [&](int f) { return sval(f, p, z); };
+                    float sig = syz_old;
+                    if (upd) {
+                        const float B0 = sv(0), B1 = sv(1), B2 = sv(2);
+                        const float A0 = sv(3), A1 = sv(4), A2 = sv(5), C0 = sv(6), C1 = sv(7), C2 = sv(8);
+                        const float dB = mu[0] * B0 + mu[1] * B1 + mu[2] * B2, qB = mu[3] * B0 + mu[4] * B1;
+                        const float dA = mu[0] * A0 + mu[1] * A1 + mu[2] * A2, qA = mu[3] * A0 + mu[4] * A1;
+                        const float dC = mu[0] * C0 + mu[1] * C1 + mu[2] * C2, qC = mu[3] * C0 + mu[4] * C1;
+                        const float Qyz = qA + qC;
+                        const float Lyz = (Qyz - qyz_old) * inv_dt;
+                        const ShearTerm tB = shear_term(2, true, p, y, z);
+                        const ShearTerm tA = shear_term(3, false, p, y, z), tC = shear_term(3, true, p, y, z);
+                        const float phB = shear_ph(tB, dB, qB), phA = shear_ph(tA, dA, qA), phC = shear_ph(tC, dC, qC);
+                        const float nxy = sxy_a + dt * (dB + phB) + qB;  // the A part is in sxy_a, qxy_a
+                        sig = sig + dt * (dA + phA + dC + phC + Lyz);
+                        qxy[ip] = qxy_a + qB;
+                        sxy[ip] = nxy;
+                        qyz[ip] = Qyz;
+                        syz[ip] = sig;
+                        shear_store(tB, qB, phB);
+                        shear_store(tA, qA, phA);
+                        shear_store(tC, qC, phC);
+                    }
+                    if constexpr (!NOD) D[(2 * P + p) * np1 + z] = sig;
                 }
             }
         }
@@ -649,7 +793,17 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N)) k_sigma
         const float inv_n = 1.0f / n;
         auto load = [&](int pp, int i) -> float2 {
             const int f = pp / Qp, q = pp - f * Qp;
-            return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
+            if constexpr (NOD) {
+                // the stresses this block stored above (the old value where
+                // the update leaves a cell), visible after the barrier that
+                // ended the last group
+                if (RAG && 2 * q >= yv) return make_float2(0.f, 0.f);
+                const float* sf = k.s[f == 0 ? 2 : f == 1 ? 4 : 5];
+                const int b = cell(k, x, y0 + 2 * q, i);
+                return make_float2(sf[b], sf[b + n]);
+            } else {
+                return make_float2(D[(f * P + 2 * q) * np1 + i], D[(f * P + 2 * q + 1) * np1 + i]);
+            }
         };
         // in place with two stages there is no B: D serves (it is read only by
         // stage 0)
@@ -1224,13 +1378,15 @@ size_t smem_mx(const KP& k, int P)
 // S[9][P][nz+1] | D[3][P][nz+1] | z tables [4][nz] | y tables [4][P] | Fz, Bz.
 // In place (compile-time lengths): tw | A | B (more than two stages) | D |
 // tables; the real fields live in the buffer the last C2R stage reads.
-size_t smem_sigma(const KP& k, int P, bool inplace)
+// Two-stage lengths (nod) leave D out: the z pass parks its results in A.
+// inplace: the compile-time path (sigma_inplace); nod: no z-pass stress buffer
+size_t smem_sigma(const KP& k, int P, bool inplace, bool nod = false)
 {
     const size_t bufA = (size_t)9 * (P / 2) * (k.nz + k.nz / 16);
     const int nb = k.pz.nst > 2 ? 2 : 1;
     const size_t sreal = inplace ? 0 : (size_t)9 * P * (k.nz + 1);
-    return sizeof(float2) * (k.nz + nb * bufA + 2 * k.nz) +
-           sizeof(float) * (sreal + (size_t)3 * P * (k.nz + 1) + 4 * k.nz + 4 * P);
+    const size_t dbuf = nod ? 0 : (size_t)3 * P * (k.nz + 1);
+    return sizeof(float2) * (k.nz + nb * bufA + 2 * k.nz) + sizeof(float) * (sreal + dbuf + 4 * k.nz + 4 * P);
 }
 
 size_t smem_vyx(int n, int P) { return sizeof(float2) * (2 * n + 2 * (n + n / 16) * P); }
@@ -1426,7 +1582,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     dispatch_len(len(k.nz, Ps, kSigmaRows), [&](auto NN) {
         constexpr int N = decltype(NN)::value;
         const dim3 grid(cdiv(k.ny, Ps), k.nx);
-        const size_t sm = smem_sigma(k, Ps, sigma_inplace(N));
+        const size_t sm = smem_sigma(k, Ps, sigma_inplace(N), sigma_nod_ok(N));
         // the runtime path's tile divides ny; a compiled length may be ragged
         if constexpr (N > 0) {
             if (k.ny % Ps) {
@@ -1452,7 +1608,9 @@ size_t step_smem_bytes(const KP& k)
     m = std::max(m, smem_fz(k, T.fz));
     m = std::max(m, smem_cy(k, T.cy, true));
     m = std::max(m, smem_mx(k, T.mx));
-    m = std::max(m, smem_sigma(k, T.sigma, false));  // the larger layout
+    // the layout launch_step takes: in place and three groups on the
+    // compile-time path, without the z pass's stress buffer at two stages
+    m = std::max(m, smem_sigma(k, T.sigma, ct_length(k.nz), ct_length(k.nz) && k.pz.nst == 2));
     return m;
 }
 

@@ -14,6 +14,9 @@ too large to compare field by field:
 * ``vti512_crop128`` -- the same crop of the 512 x 512 x 256 model of the
   precision configuration (the generator at that size, seed 2024; its dt
   from that model's stability bound), 400 steps.
+* ``config1_force_planes`` -- the small configuration with the reference's
+  own force source, the FP64 counterpart of the reference-build fixture
+  tests/golden/config1.npz (planes 12 cells beside the source).
 * ``config1_explosive`` -- the small isotropic configuration as specified
   (96^3, 20-cell C-PML, Vp 2500, Vs 1443, rho 2000, Qp 100, Qs 50, 25 Hz,
   dt 1 ms, 500 steps) with the explosive source at the grid centre, which the
@@ -92,9 +95,20 @@ def config1_explosive_case(nt=500):
     return c
 
 
+def config1_force_planes_case(nt=500):
+    """The small configuration with the reference's own source (force on vx at
+    s_iz + 10, the centre), as in tests/golden/config1.npz from the
+    reference's cuFFT build: the FP64 result on the x-z plane 12 cells
+    beside the source (vy is antisymmetric about the source's own plane)."""
+    c = qc.config1_case(nt=nt)
+    c["name"] = "config1_force_planes"
+    c.update(vti=0, src_type=0, ref_offset=1, plane_y=60, plane_z=-1)
+    return c
+
+
 def cases():
     return {"vti_crop128": vti_crop128_case, "config1_explosive": config1_explosive_case,
-            "vti512_crop128": vti512_crop128_case}
+            "vti512_crop128": vti512_crop128_case, "config1_force_planes": config1_force_planes_case}
 
 
 def model_sums(c):
@@ -106,16 +120,25 @@ def save_case(outdir, c):
     import oracle
     snaps = list(range(100, int(c["nt"]) + 1, 100))
     t0 = time.time()
-    r = oracle.run_case(c, snaps=snaps, src_type=int(c["src_type"]), vti=bool(c["vti"]), ref_offset=False)
+    r = oracle.run_case(c, snaps=snaps, src_type=int(c["src_type"]), vti=bool(c["vti"]),
+                        ref_offset=bool(c.get("ref_offset", 0)))
+    write_case(outdir, c, r)
+    print("oracle %.0f s" % (time.time() - t0), flush=True)
+
+
+def write_case(outdir, c, r):
+    """The fixture of case c from an oracle run r (run_case's result)."""
+    snaps = list(range(100, int(c["nt"]) + 1, 100))
     out = {k: np.asarray(v) for k, v in c.items() if k not in MODEL_KEYS}
     out["model_sums"] = model_sums(c)
     out["rec_vx"], out["rec_vy"], out["rec_vz"] = r["rec"]
     for k in snaps:
         out["plane_y_%d" % k] = r["snaps"][k][:, :, int(c["plane_y"]), :].copy()
-        out["plane_z_%d" % k] = r["snaps"][k][:, :, :, int(c["plane_z"])].copy()
+        if int(c["plane_z"]) >= 0:
+            out["plane_z_%d" % k] = r["snaps"][k][:, :, :, int(c["plane_z"])].copy()
     path = os.path.join(outdir, c["name"] + ".npz")
     np.savez_compressed(path, **out)
-    print("wrote %s (oracle %.0f s)" % (path, time.time() - t0), flush=True)
+    print("wrote %s" % path, flush=True)
 
 
 def main():

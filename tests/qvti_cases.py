@@ -115,3 +115,27 @@ def relL2(a, b):
     b = np.asarray(b, np.float64)
     nb = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / nb) if nb > 0 else float(np.linalg.norm(a - b))
+
+
+def snapshot_error(ours, ref, peak):
+    """Error of one field of a snapshot plane against its reference: relative
+    L2, except where the reference field is below 1 % of `peak` -- the
+    largest norm of the whole wavefield (vx, vy, vz together) on that plane
+    over the run -- where the L2 error is taken relative to that peak
+    instead.  Two cases reach it: a component that vanishes by symmetry on
+    the plane (vy through an x-directed or an explosive source), and a
+    field that has decayed after the wave left through the C-PML.  There
+    relative L2 measures FP32 rounding, not the scheme: the reference's own
+    cuFFT build differs from the FP64 oracle by 1.1e-3 relative L2 on the
+    96^3 configuration's plane at step 500, where the field is 5e-4 of its
+    peak, against 2.5e-6..1.7e-5 at steps 100-400."""
+    a = np.asarray(ours, np.float64)
+    b = np.asarray(ref, np.float64)
+    nb = np.linalg.norm(b)
+    d = np.linalg.norm(a - b)
+    return d / max(nb, 1e-2 * peak) if peak > 0 else d
+
+
+def plane_peak(planes):
+    """Largest norm of a wavefield plane ([3, ...] per snapshot) over a run."""
+    return max(float(np.linalg.norm(np.asarray(p, np.float64))) for p in planes)

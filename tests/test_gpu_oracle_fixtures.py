@@ -8,9 +8,15 @@ reference's cuFFT build in tests/test_oracle.py).
   C-PML, strong heterogeneity and anisotropy over a long run).
 * config1_explosive: 96^3 isotropic, explosive source at the centre, 500
   steps.
+* config1_force_planes: the same grid with the reference's force source,
+  the FP64 counterpart of the reference-build fixture tests/golden/config1.npz.
 
 Tolerance: relative L2 <= 1e-4 on every seismogram component and on the vx,
-vy, vz planes of every snapshot (every 100 steps).
+vy, vz planes of every snapshot (every 100 steps), each field relative to
+its own norm unless that is below 1 % of the wavefield's peak on the plane
+over the run (a component that vanishes there by symmetry, or a field
+after the wave has left), then relative to that peak
+(qvti_cases.snapshot_error).
 """
 import os
 import sys
@@ -59,19 +65,22 @@ def test_against_oracle_fixture(qvti, name):
     c, g = _case(name)
     nt = int(c["nt"])
     snaps = list(range(100, nt + 1, 100))
-    ours = qvti.run_case(c, snaps=snaps, src_type=int(c["src_type"]), vti=bool(c["vti"]), ref_offset=False)
+    ours = qvti.run_case(c, snaps=snaps, src_type=int(c["src_type"]), vti=bool(c["vti"]),
+                         ref_offset=bool(c.get("ref_offset", 0)))
     worst = 0.0
     for i, comp in enumerate(("vx", "vy", "vz")):
         e = qc.relL2(ours["rec"][i], g["rec_" + comp])
         worst = max(worst, e)
         assert e <= TOL, "%s seismogram %s relL2 %.3g" % (name, comp, e)
     py, pz = int(c["plane_y"]), int(c["plane_z"])
-    for k in snaps:
-        f = ours["snaps"][k]
+    for lab in ("y", "z") if pz >= 0 else ("y",):
+        peak = qc.plane_peak([g["plane_%s_%d" % (lab, k)] for k in snaps])
         for i in range(3):
-            for lab, mine, ref in (("y", f[i][:, py, :], g["plane_y_%d" % k][i]),
-                                   ("z", f[i][:, :, pz], g["plane_z_%d" % k][i])):
-                e = qc.relL2(mine, ref)
+            ref = [g["plane_%s_%d" % (lab, k)][i] for k in snaps]
+            for k, r in zip(snaps, ref):
+                f = ours["snaps"][k][i]
+                mine = f[:, py, :] if lab == "y" else f[:, :, pz]
+                e = qc.snapshot_error(mine, r, peak)
                 worst = max(worst, e)
-                assert e <= TOL, "%s step %d field %d plane %s relL2 %.3g" % (name, k, i, lab, e)
-    print("%s worst relL2 %.2e" % (name, worst))
+                assert e <= TOL, "%s step %d field %d plane %s error %.3g" % (name, k, i, lab, e)
+    print("%s worst error %.2e" % (name, worst))
