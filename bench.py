@@ -360,6 +360,8 @@ def our_arm(args, world, rank, local):
     src = (nx // 2, ny // 2, PML + 5)
 
     sim = qv.Simulation(nx, ny, nz, PML, DX, DX, DX, dt, F0, vti=True, device=local)
+    if args.form == "tc":
+        sim.set_form(qv.FORM_TC)
     sim.set_model(model["velp"], model["vels"], model["rho"], model["gama_p"], model["gama_s"],
                   model["eps"], model["delta"])
     sim.set_receivers(PML, r_ix, r_iy)
@@ -698,6 +700,10 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's cuFFT build")
     ap.add_argument("--no-tc", action="store_true", help="skip the tensor-core form")
     ap.add_argument("--grid", type=int, default=256, help="cube edge (profiling of smaller cases)")
+    ap.add_argument("--ny", type=int, default=0, help="y length other than --grid (profiling of smaller cases)")
+    ap.add_argument("--form", default="plain", choices=["plain", "tc"],
+                    help="form of the timed steps (profiling; the default line times the plain form and "
+                         "reports the tensor-core form beside it)")
     ap.add_argument("--workload", default="step", choices=["step", "batch", "serve", "precision"])
     ap.add_argument("--nt", type=int, default=3000, help="precision: steps of the 512x512x256 run")
     ap.add_argument("--shots", type=int, default=48, help="batch: number of shots")
@@ -714,10 +720,10 @@ def main():
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = dist_setup()
-    if args.grid != 256:
+    if args.grid != 256 or args.ny:
         global GRID, PML
-        GRID = (args.grid,) * 3
-        PML = min(30, max(4, args.grid // 8))
+        GRID = (args.grid, args.ny or args.grid, args.grid)
+        PML = min(30, max(4, min(GRID) // 8))
     if args.impl == "reference":
         return reference_arm(args, world, rank)
     return our_arm(args, world, rank, local)

@@ -233,6 +233,55 @@ enum { QVTI_FORM_PLAIN = 0, QVTI_FORM_TC = 1 };
 int qvti_set_form(qvti_sim* sim, int form);
 
 /* ---------------------------------------------------------------------
+ * Reverse-time migration and Q compensation.  The reference declares these
+ * as flags only (viscoelas_3D.cpp:1-3 "viscoacoustic reverse time
+ * migration", :42-65 RTM_type, imaging_condition, media_type, :223-229
+ * checkpoints) and implements none of them.
+ * --------------------------------------------------------------------- */
+enum {
+    QVTI_MEDIA_VISCOELASTIC = 1,   /* dispersion and loss (the default)                    */
+    QVTI_MEDIA_DISPERSION_ONLY = 2, /* constant-Q dispersion, loss terms off                */
+    QVTI_MEDIA_LOSSLESS = 3,        /* gamma = 0: elastic (built by qvti_set_model)         */
+    QVTI_MEDIA_Q_COMPENSATED = 4    /* loss terms with reversed sign: amplitude compensation
+                                       for back-propagation (unstable over long distances at
+                                       high frequency, as any amplitude-amplifying operator) */
+};
+/* Medium of the stepping (viscoelas_3D.cpp:59-63's media_type).  Call before
+ * qvti_set_model (the lossless medium changes the coefficients it builds). */
+int qvti_set_media(qvti_sim* sim, int media);
+
+/* Back-propagation source: from the next step on, step it adds sample
+ * nt - 1 - it of each given component (host arrays of nt x rn floats,
+ * [it][ir] like the records; any may be NULL) to that velocity component at
+ * receiver ir, where the records are taken (the adjoint of recording).  Set
+ * after qvti_set_receivers; nt = 0 clears it. */
+int qvti_set_injection(qvti_sim* sim, const float* vx, const float* vy, const float* vz, int nt);
+
+typedef struct {
+    int media;        /* QVTI_MEDIA_* of both propagations                          */
+    int snap_every;   /* imaging interval: correlate every snap_every-th step      */
+    float illum_eps;  /* source-normalised image: I / (illumination + eps max illum) */
+} qvti_rtm_opts;
+
+/* One shot of reverse-time migration: the source wavefield is propagated
+ * forward and its velocities kept on the device every opts->snap_every steps;
+ * the observed records (nt x rn per component; NULL components are not
+ * injected) are propagated backward in time from the receivers; at the kept
+ * steps the zero-lag cross-correlation image sum_t sum_c S_c R_c
+ * (imaging_condition 4) and the source illumination sum_t sum_c S_c^2 are
+ * accumulated on the device.  image_xcorr and image_norm (the cross-
+ * correlation divided by the illumination plus opts->illum_eps times its
+ * maximum, imaging_condition 3) receive ntx*nty*ntz floats each (either may
+ * be NULL).  QVTI_ERR_OOM if the kept source velocities do not fit;
+ * QVTI_ERR_NONFINITE if a propagation blew up (the Q-compensated medium
+ * over long paths through strong attenuation). */
+int qvti_rtm_shot(const qvti_config* cfg, const float* velp, const float* vels, const float* rho, const float* gama_p,
+                  const float* gama_s, const float* eps, const float* delta, int src_type, int s_ix, int s_iy, int s_iz,
+                  const float* wavelet, int nt, int r_iz, const int* r_ix, const int* r_iy, int rn,
+                  const float* obs_vx, const float* obs_vy, const float* obs_vz, const qvti_rtm_opts* opts,
+                  float* image_xcorr, float* image_norm);
+
+/* ---------------------------------------------------------------------
  * Batches and serving.  The reference runs shots one after another from a
  * host loop (viscoelas_3D.cpp:355-405, one cuda_forward_acoustic_3D call per
  * shot, cuviscoelas_3D.cu:1163-1629); these entry points run many shots of

@@ -196,6 +196,9 @@ struct Sim {
     double* d_norm = nullptr;
     int* d_bad = nullptr;
     int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
+    int media = QVTI_MEDIA_VISCOELASTIC;
+    float* d_inj[3] = {};  // time-reversed traces (qvti_set_injection)
+    size_t inj_cap[3] = {};
     int* d_nonfinite = nullptr;  // set by qvti_check_finite_async
     int nt = 0, rn = 0;
     bool have_model = false, have_src = false;
@@ -413,6 +416,11 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.dft16 = dft16;
     k.err = s->d_err;
     k.form = kFormPlain;
+    k.loss_scale = 1.0f;
+    k.sigma_pf = 0;
+    if (const char* e = getenv("QVTI_SIGMA_PF")) k.sigma_pf = atoi(e) ? 1 : 0;
+    k.inj[0] = k.inj[1] = k.inj[2] = nullptr;
+    k.inj_nt = 0;
 
 
     for (int j = 0; j < 5; ++j) k.MU[j] = mu[j];
@@ -490,7 +498,7 @@ extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels,
     QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 12, cudaMemcpyHostToDevice, s->st));
     const float w0 = s->kp.w0;
     launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
-                      s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, w0, d_coef, s->st);
+                      s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, w0, s->media == QVTI_MEDIA_LOSSLESS, d_coef, s->st);
     launch_mu_rinv(s->kp, dev[2], s->coef + 7, s->st);
     QV_CUDA(cudaGetLastError());
     QV_CUDA(cudaStreamSynchronize(s->st));
@@ -1001,6 +1009,45 @@ extern "C" int qvti_set_kz_batch(qvti_sim* s, int kz_batch)
         s->kp.kz_batch = kz_batch;
         if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_media(qvti_sim* s, int media)
+{
+    using namespace qvti;
+    if (!s || media < QVTI_MEDIA_VISCOELASTIC || media > QVTI_MEDIA_Q_COMPENSATED) return fail(QVTI_ERR_ARG);
+    s->media = media;
+    const float ls = media == QVTI_MEDIA_VISCOELASTIC ? 1.0f : media == QVTI_MEDIA_Q_COMPENSATED ? -1.0f : 0.0f;
+    if (s->kp.loss_scale != ls) {
+        s->kp.loss_scale = ls;
+        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    }
+    // the lossless medium's coefficients are built without gamma: a model
+    // set before this call is out of date
+    s->have_model = false;
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_injection(qvti_sim* s, const float* vx, const float* vy, const float* vz, int nt)
+{
+    using namespace qvti;
+    if (!s || nt < 0 || (nt > 0 && !vx && !vy && !vz)) return fail(QVTI_ERR_ARG);
+    if (nt > 0 && s->rn <= 0) return fail(QVTI_ERR_STATE);  // injected at the receivers
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    const float* host[3] = {vx, vy, vz};
+    KP& k = s->kp;
+    for (int c = 0; c < 3; ++c) {
+        k.inj[c] = nullptr;
+        if (nt == 0 || !host[c]) continue;
+        const size_t n = (size_t)nt * s->rn;
+        if (s->ensure(&s->d_inj[c], &s->inj_cap[c], n)) return g_last_error;
+        QV_CUDA(cudaMemcpyAsync(s->d_inj[c], host[c], sizeof(float) * n, cudaMemcpyHostToDevice, s->st));
+        k.inj[c] = s->d_inj[c];
+    }
+    k.inj_nt = nt;
+    QV_CUDA(cudaStreamSynchronize(s->st));
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     return QVTI_OK;
 }
 

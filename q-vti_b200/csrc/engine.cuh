@@ -106,6 +106,14 @@ struct KP {
     int form;
     const float* dft16;  // tensor-core DFT matrices (k_dft16_tables), null if unused
     int* err;            // device error flag (a bounded wait that gave up), 0 = ok
+    // medium: scale of the constant-Q loss terms (1 viscoelastic, 0
+    // dispersion only or lossless, -1 Q-compensated back-propagation)
+    float loss_scale;
+    // time-reversed traces added at the receivers (nt_inj x rn each; null:
+    // none), the adjoint source of back-propagation
+    const float* inj[3];
+    int inj_nt;
+    int sigma_pf;  // k_sigma: prefetch the next group's half spectra into L2 (tuning experiment)
 };
 constexpr int kFormPlain = 0, kFormTc = 1;
 
@@ -156,7 +164,7 @@ constexpr size_t kMaxSmem = 226 * 1024;  // dynamic; an SM block takes 227 KB wi
 // (input of the MU average).
 void launch_coef_build(const KP& kp, const float* velp, const float* vels, const float* rho,
                        const float* gp, const float* gs, const float* eps, const float* delta, int vti,
-                       float w0, float* const* coef_out, cudaStream_t st);
+                       float w0, int lossless, float* const* coef_out, cudaStream_t st);
 void launch_mu_rinv(const KP& kp, const float* rho, const float* const* sset, cudaStream_t st);
 int configure_kernels();   // raise dynamic shared-memory limits, returns cudaError_t
 // configure_kernels() once per device (the device must be current); 0 = ok.

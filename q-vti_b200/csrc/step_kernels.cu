@@ -382,7 +382,10 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
     __syncthreads();
     const int it = *k.d_it;
     const float inv_nz = 1.0f / n;
-    const float dt = k.dt, inv_dt = 1.0f / k.dt;
+    // inv_dt enters only the loss terms (the spectral time derivative of the
+    // constant-Q loss operator): their sign and presence follow the medium
+    // (k.loss_scale: 1 viscoelastic, 0 dispersion only, -1 Q-compensated)
+    const float dt = k.dt, ls = k.loss_scale, inv_dt = ls / k.dt;
     const float w0 = k.w0, inv_w0 = 1.0f / k.w0;
     const int src_ip = (k.s_ix >= 0) ? cell(k, k.s_ix, k.s_iy, k.s_iz) : -1;
 
@@ -450,6 +453,18 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
         const int o0 = REGRP ? 9 * grp : grp == 0 ? 0 : 9 + (grp - 1) * 6;
         const int npen = NF * Qp;
         prefetch_group(grp + 1);
+        if (k.sigma_pf && grp + 1 < NGRP) {
+            // the next group's half spectra into L2: one 8 P-byte run (the
+            // tile's P rows) per field and kz, spread over the threads
+            const int nf1 = (REGRP || grp + 1 == 0) ? 9 : 6;
+            const int o1 = REGRP ? 9 * (grp + 1) : 9 + grp * 6;
+            const int nkz = n / 2 + 1;
+            for (int idx = threadIdx.x; idx < nf1 * nkz; idx += blockDim.x) {
+                const int f = idx / nkz, kz = idx - f * nkz;
+                const float2* a = s_src[o1 + f] + spec(k, kz, x, y0);
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+            }
+        }
         // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
@@ -699,9 +714,10 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
                 }
             } else if (grp == 1) {
                 // xz, and the A half (dy vx: y slab) of xy: with
-                // dt L = Qxy - Qxy_old, sxy_new = sxy + dt (dA + phA) + qA - Qxy_old
-                // + dt (dB + phB) + qB and Qxy_new = qA + qB; the A part goes
-                // into the stored sxy and Qxy now, the B part in the next group
+                // dt L = ls (Qxy - Qxy_old), sxy_new = sxy + dt (dA + phA) +
+                // ls (qA - Qxy_old) + dt (dB + phB) + ls qB and Qxy_new = qA + qB;
+                // the A part goes into the stored sxy and Qxy now, the B part
+                // in the next group
                 float* __restrict__ sg = k.s[4];
                 float* __restrict__ qg = k.Q[4];
                 float* __restrict__ sxy = k.s[3];
@@ -735,7 +751,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
                         shear_store(tA, qA, phA);
                         shear_store(tB, qB, phB);
                         shear_store(tC, qC, phC);
-                        sxy[ip] = sxy_old + dt * (dC + phC) + (qC - qxy_old);
+                        sxy[ip] = sxy_old + dt * (dC + phC) + ls * (qC - qxy_old);
                         qxy[ip] = qC;
                     }
                     if constexpr (!NOD) D[(1 * P + p) * np1 + z] = sig;
@@ -769,7 +785,7 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
                         const ShearTerm tB = shear_term(2, true, p, y, z);
                         const ShearTerm tA = shear_term(3, false, p, y, z), tC = shear_term(3, true, p, y, z);
                         const float phB = shear_ph(tB, dB, qB), phA = shear_ph(tA, dA, qA), phC = shear_ph(tC, dC, qC);
-                        const float nxy = sxy_a + dt * (dB + phB) + qB;  // the A part is in sxy_a, qxy_a
+                        const float nxy = sxy_a + dt * (dB + phB) + ls * qB;  // the A part is in sxy_a, qxy_a
                         sig = sig + dt * (dA + phA + dC + phC + Lyz);
                         qxy[ip] = qxy_a + qB;
                         sxy[ip] = nxy;
@@ -1155,16 +1171,27 @@ __global__ void __launch_bounds__(kThreads) k_vx(KP k, int P_rt)
 }
 
 // ----------------------------------------------------------------- k_rec --
+// Receivers (cu:782-791).  With traces to inject (back-propagation of
+// recorded data, the adjoint of recording), sample nt - 1 - it of each
+// component is first added to that component at the receiver, at the point
+// of the step where the source is injected and the records are taken.
 __global__ void k_rec(KP k)
 {
     const int ir = blockIdx.x * blockDim.x + threadIdx.x;
     const int it = *k.d_it;
     if (ir >= k.rn || it < 0 || it >= k.nt_rec) return;
     const int ip = cell(k, k.r_ix[ir], k.r_iy[ir], k.r_iz);
+    if (it < k.inj_nt) {
+        const long long o = (long long)(k.inj_nt - 1 - it) * k.rn + ir;
+        for (int c = 0; c < 3; ++c)
+            if (k.inj[c]) k.v[c][ip] += k.inj[c][o];
+    }
     const long long o = (long long)it * k.rn + ir;
-    k.rec[0][o] = k.v[0][ip];
-    k.rec[1][o] = k.v[1][ip];
-    k.rec[2][o] = k.v[2][ip];
+    if (k.rec[0]) {
+        k.rec[0][o] = k.v[0][ip];
+        k.rec[1][o] = k.v[1][ip];
+        k.rec[2][o] = k.v[2][ip];
+    }
 }
 
 // ----------------------------------------------------- setup, FP64 kernels --
@@ -1192,12 +1219,16 @@ __device__ __forceinline__ void qset(double v, double g, double r, double w0, do
 // sets are P(v) - 2 S(vs), which at eps = delta = 0 is the reference's
 // eta_p - 2 eta_s (cu:851-898).
 __global__ void k_coef(long long ntp, const float* velp, const float* vels, const float* rho, const float* gp,
-                       const float* gs, const float* eps, const float* delta, int vti, double w0, float* const* out)
+                       const float* gs, const float* eps, const float* delta, int vti, double w0, int lossless,
+                       float* const* out)
 {
     const double pi = 3.1415926;
     for (long long ip = blockIdx.x * (long long)blockDim.x + threadIdx.x; ip < ntp;
          ip += (long long)gridDim.x * blockDim.x) {
-        const double r = rho[ip], vp = velp[ip], vs = vels[ip], g_p = gp[ip], g_s = gs[ip];
+        // lossless medium: gamma = 0 (Q infinite), the constant-Q sets reduce
+        // to the elastic moduli
+        const double r = rho[ip], vp = velp[ip], vs = vels[ip], g_p = lossless ? 0.0 : gp[ip],
+                     g_s = lossless ? 0.0 : gs[ip];
         const double cp = cos(g_p * pi / 2.0), cq = cos(g_s * pi / 2.0);
         double v11 = vp, v13 = vp;
         if (vti) {
@@ -1615,10 +1646,10 @@ size_t step_smem_bytes(const KP& k)
 }
 
 void launch_coef_build(const KP& k, const float* velp, const float* vels, const float* rho, const float* gp,
-                       const float* gs, const float* eps, const float* delta, int vti, float w0, float* const* coef_out,
-                       cudaStream_t st)
+                       const float* gs, const float* eps, const float* delta, int vti, float w0, int lossless,
+                       float* const* coef_out, cudaStream_t st)
 {
-    k_coef<<<148 * 8, 256, 0, st>>>(k.ntp, velp, vels, rho, gp, gs, eps, delta, vti, (double)w0, coef_out);
+    k_coef<<<148 * 8, 256, 0, st>>>(k.ntp, velp, vels, rho, gp, gs, eps, delta, vti, (double)w0, lossless, coef_out);
 }
 
 void launch_mu_rinv(const KP& k, const float* rho, const float* const* sset, cudaStream_t st)

@@ -19,6 +19,7 @@ SRC_FORCE_X = 0
 SRC_EXPLOSIVE = 1
 FORM_PLAIN = 0  # every transform stage as FP32 butterflies
 FORM_TC = 1     # 256-point y transforms as split-precision tensor-core contractions
+MEDIA_VISCOELASTIC, MEDIA_DISPERSION_ONLY, MEDIA_LOSSLESS, MEDIA_Q_COMPENSATED = 1, 2, 3, 4
 FIELDS = ("vx", "vy", "vz", "pxx", "pyy", "pzz", "pxy", "pxz", "pyz")
 
 
@@ -53,6 +54,10 @@ class Shot(ctypes.Structure):
 class ShotResult(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("queue_s", ctypes.c_double), ("latency_s", ctypes.c_double),
                 ("device_ms", ctypes.c_float)]
+
+
+class RtmOpts(ctypes.Structure):
+    _fields_ = [("media", ctypes.c_int), ("snap_every", ctypes.c_int), ("illum_eps", ctypes.c_float)]
 
 
 class SchedOpts(ctypes.Structure):
@@ -107,6 +112,11 @@ def lib():
             "qvti_get_stream": (ctypes.c_int, [_V, ctypes.POINTER(_V)]),
             "qvti_set_kz_batch": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_set_form": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_set_media": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_set_injection": (ctypes.c_int, [_V, _F, _F, _F, ctypes.c_int]),
+            "qvti_rtm_shot": (ctypes.c_int, [ctypes.POINTER(Config), _F, _F, _F, _F, _F, _F, _F, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int,
+                                             _I, _I, ctypes.c_int, _F, _F, _F, ctypes.POINTER(RtmOpts), _F, _F]),
             "qvti_server_create": (ctypes.c_int, [ctypes.POINTER(SchedOpts), ctypes.POINTER(_V)]),
             "qvti_server_submit": (ctypes.c_int, [_V, ctypes.POINTER(Shot), ctypes.POINTER(ctypes.c_longlong)]),
             "qvti_server_wait": (ctypes.c_int, [_V, ctypes.c_longlong, ctypes.c_double,
@@ -210,6 +220,17 @@ class Simulation:
         """FORM_PLAIN or FORM_TC (qvti_set_form)."""
         _check(lib().qvti_set_form(self._h, int(form)), "qvti_set_form")
 
+    def set_media(self, media):
+        """MEDIA_* (qvti_set_media); call before set_model."""
+        _check(lib().qvti_set_media(self._h, int(media)), "qvti_set_media")
+
+    def set_injection(self, vx=None, vy=None, vz=None):
+        """Time-reversed traces ([nt, rn] each, any may be None) added at the
+        receivers from the next step on (qvti_set_injection)."""
+        arrs = [None if a is None else _f32(a) for a in (vx, vy, vz)]
+        nt = next(a.shape[0] for a in arrs if a is not None)
+        _check(lib().qvti_set_injection(self._h, *[_fp(a) for a in arrs], int(nt)), "qvti_set_injection")
+
     def reset(self):
         _check(lib().qvti_reset(self._h), "qvti_reset")
 
@@ -302,23 +323,52 @@ def q_derivative_noalloc(d_in, d_out, shape, spacing, axis, forward, power, stre
            "qvti_q_derivative_noalloc")
 
 
+def rtm_shot(c, obs, media=MEDIA_VISCOELASTIC, snap_every=5, illum_eps=1e-3, vti=False, src_type=SRC_FORCE_X,
+             ref_offset=True, device=0):
+    """Reverse-time migration of one shot (qvti_rtm_shot): case c gives the
+    migration model, source and receivers; obs = [3, nt, rn] observed records
+    (None entries are not injected).  Returns (cross-correlation image,
+    source-normalised image), each [ntx, nty, ntz]."""
+    shape = (int(c["ntx"]), int(c["nty"]), int(c["ntz"]))
+    keep = [_f32(c[k], shape) for k in ("velp", "vels", "rho", "gama_p", "gama_s")]
+    keep += [_f32(c["eps"], shape), _f32(c["delta"], shape)] if vti else [None, None]
+    rik = _f32(c["rik"])
+    nt = rik.size
+    rx = np.ascontiguousarray(c["r_ix"], np.int32)
+    ry = np.ascontiguousarray(c["r_iy"], np.int32)
+    ob = [None if o is None else _f32(o) for o in obs]
+    cfg = Config(*shape, int(c["pml"]), float(c["dx"]), float(c["dy"]), float(c["dz"]), float(c["dt"]),
+                 float(c["f0"]), 1 if vti else 0, int(device), 0.0)
+    opts = RtmOpts(int(media), int(snap_every), float(illum_eps))
+    im = np.zeros(shape, np.float32)
+    imn = np.zeros(shape, np.float32)
+    _check(lib().qvti_rtm_shot(ctypes.byref(cfg), *[_fp(a) for a in keep], int(src_type), int(c["s_ix"]),
+                               int(c["s_iy"]), int(c["s_iz"]) + (10 if ref_offset else 0), _fp(rik), nt,
+                               int(c["r_iz"]), rx.ctypes.data_as(_I), ry.ctypes.data_as(_I), rx.size,
+                               *[_fp(o) for o in ob], ctypes.byref(opts), _fp(im), _fp(imn)), "qvti_rtm_shot")
+    return im, imn
+
+
 def simulation_for_case(c, vti=False, device=0):
     return Simulation(c["ntx"], c["nty"], c["ntz"], c["pml"], c["dx"], c["dy"], c["dz"], c["dt"], c["f0"],
                       vti=vti, device=device)
 
 
 def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=True, device=0, want_state=False,
-             form=FORM_PLAIN):
+             form=FORM_PLAIN, media=MEDIA_VISCOELASTIC):
     """Run a shot described by a case dict (tests/qvti_cases.py conventions).
 
     Returns dict(rec=[3, nt, rn], snaps={k: [3, ...]}, state=[9, ...] or None).
     ``ref_offset`` adds the reference's +10 to s_iz (cuviscoelas_3D.cu:772);
-    ``form`` selects the transforms' form (FORM_PLAIN, FORM_TC)."""
+    ``form`` selects the transforms' form (FORM_PLAIN, FORM_TC), ``media``
+    the medium (MEDIA_*)."""
     nt = int(c["nt"] if nt is None else nt)
     snaps = sorted(int(s) for s in snaps)
     with simulation_for_case(c, vti=vti, device=device) as sim:
         if form != FORM_PLAIN:
             sim.set_form(form)
+        if media != MEDIA_VISCOELASTIC:
+            sim.set_media(media)
         sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"],
                       c.get("eps") if vti else None, c.get("delta") if vti else None)
         sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])
