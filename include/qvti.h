@@ -343,10 +343,22 @@ int qvti_server_destroy(qvti_server* srv);
 int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_opts* opts, qvti_shot_result* results,
                    double* wall_s);
 
-/* Probe one grid: run probe_steps steps on 1..max_active concurrent
- * simulations (homogeneous model) for each kz batch in {nz/2+1, (nz/2+2)/2}
- * and report the fastest setting and its Gcell-steps/s.  The scheduler
- * caches the result per grid. */
+/* Probe one grid: the form of the transforms (plain FP32 stages, or the
+ * tensor-core DFT plan where the grid has one) with one shot in flight, then
+ * probe_steps steps on 1..max_active concurrent simulations (homogeneous
+ * model) for each kz batch in {nz/2+1, (nz/2+2)/2}; report the fastest
+ * setting and its Gcell-steps/s.  The scheduler caches the result per grid
+ * and applies it to the shots of that grid.  No counterpart in the
+ * reference, which runs one shot at a time (viscoelas_3D.cpp:355-405). */
+typedef struct {
+    int active;          /* shots in flight                                   */
+    int kz_batch;        /* kz planes per batch of the k-space passes         */
+    int form;            /* QVTI_FORM_PLAIN or QVTI_FORM_TC                   */
+    double gcell_steps;  /* measured Gcell-steps/s of that setting            */
+} qvti_tuning;
+int qvti_autotune_ex(const qvti_config* cfg, int max_active, int probe_steps, qvti_tuning* best);
+
+/* qvti_autotune_ex without the form in the result. */
 int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active, int* best_kz_batch,
                   double* gcell_steps);
 

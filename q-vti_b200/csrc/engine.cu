@@ -417,8 +417,6 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.err = s->d_err;
     k.form = kFormPlain;
     k.loss_scale = 1.0f;
-    k.sigma_pf = 0;
-    if (const char* e = getenv("QVTI_SIGMA_PF")) k.sigma_pf = atoi(e) ? 1 : 0;
     k.inj[0] = k.inj[1] = k.inj[2] = nullptr;
     k.inj_nt = 0;
 

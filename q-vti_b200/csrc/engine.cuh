@@ -113,7 +113,6 @@ struct KP {
     // none), the adjoint source of back-propagation
     const float* inj[3];
     int inj_nt;
-    int sigma_pf;  // k_sigma: prefetch the next group's half spectra into L2 (tuning experiment)
 };
 constexpr int kFormPlain = 0, kFormTc = 1;
 

@@ -69,7 +69,7 @@ struct ShapeKey {
 };
 
 struct Tuning {
-    int active, kz_batch;
+    int active, kz_batch, form;
 };
 std::mutex g_tune_mu;
 std::map<ShapeKey, Tuning> g_tune;
@@ -247,7 +247,10 @@ int qvti_server::start(Job* j, PoolSim* ps)
     j->slot = ps;
     int rc;
     Tuning t;
-    if (cached_tuning({s.ntx, s.nty, s.ntz, s.vti}, &t) && (rc = qvti_set_kz_batch(sim, t.kz_batch))) return rc;
+    if (cached_tuning({s.ntx, s.nty, s.ntz, s.vti}, &t)) {
+        if ((rc = qvti_set_kz_batch(sim, t.kz_batch))) return rc;
+        if ((rc = qvti_set_form(sim, t.form))) return rc;
+    }
     if ((rc = qvti_set_model(sim, s.velp, s.vels, s.rho, s.gama_p, s.gama_s, s.eps, s.delta, 0))) return rc;
     if ((rc = qvti_set_receivers(sim, s.r_iz, s.r_ix, s.r_iy, s.rn))) return rc;
     if ((rc = qvti_set_source(sim, s.src_type, s.s_ix, s.s_iy, s.s_iz, s.wavelet, s.nt))) return rc;
@@ -490,7 +493,7 @@ extern "C" int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_op
             double g = 0;
             if (qvti_autotune(&cfg, 4, 8, &a, &b, &g) != QVTI_OK) {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
-                g_tune[k] = {1, (cfg.ntz / 2 + 1)};
+                g_tune[k] = {1, (cfg.ntz / 2 + 1), QVTI_FORM_PLAIN};
             }
         }
     }
@@ -516,11 +519,14 @@ extern "C" int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_op
 }
 
 // ------------------------------------------------------------- autotuner --
-extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active,
-                             int* best_kz_batch, double* gcell_steps)
+// Probe one grid: first the form of the transforms (the FP32 Stockham stages,
+// or the tensor-core DFT plan where the grid has one) with one shot in
+// flight, then, in that form, 1..max_active shots in flight for each kz
+// batch in {nz/2+1, (nz/2+2)/2}.  A setting must be 2 % faster than the
+// simpler one (plain form, fewer shots) to be taken.
+extern "C" int qvti_autotune_ex(const qvti_config* cfg, int max_active, int probe_steps, qvti_tuning* best_out)
 {
-    if (!cfg || max_active < 1 || probe_steps < 1 || !best_active || !best_kz_batch || !gcell_steps)
-        return QVTI_ERR_ARG;
+    if (!cfg || max_active < 1 || probe_steps < 1 || !best_out) return QVTI_ERR_ARG;
     if (cudaSetDevice(cfg->device) != cudaSuccess) return QVTI_ERR_CUDA;
     const size_t ntp = (size_t)cfg->ntx * cfg->nty * cfg->ntz;
     size_t free_b = 0, total_b = 0;
@@ -531,7 +537,8 @@ extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_s
     std::vector<float> vp(ntp, 3000.f), vs(ntp, 1700.f), rho(ntp, 2200.f);
     std::vector<float> gp(ntp, (float)(std::atan(1.0 / 100.0) / 3.1415926)), gs(ntp, (float)(std::atan(1.0 / 50.0) / 3.1415926));
     std::vector<float> eps(cfg->vti ? ntp : 0, 0.1f), dl(cfg->vti ? ntp : 0, 0.05f);
-    const int warm = 2, nt = warm + probe_steps;
+    const int warm = 2;
+    const int nt = 2 * (warm + probe_steps);  // the form probe and the concurrency probes
     std::vector<float> wav(nt, 0.f);
     wav[0] = 1.f;
     std::vector<qvti_sim*> sims;
@@ -546,35 +553,65 @@ extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_s
     }
     if (sims.empty()) return rc ? rc : QVTI_ERR_OOM;
     const int nkz = cfg->ntz / 2 + 1;
-    const int kzb[2] = {nkz, (nkz + 1) / 2};
+    // steps per second of `c` simulations, each running `steps` after a reset and `warm` steps
+    auto probe = [&](int c, int b, int form, double* rate) -> int {
+        for (int i = 0; i < c; ++i) {
+            int r;
+            if ((r = qvti_set_kz_batch(sims[i], b)) || (r = qvti_set_form(sims[i], form)) || (r = qvti_reset(sims[i])) ||
+                (r = qvti_step(sims[i], warm)))
+                return r;
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess) return QVTI_ERR_CUDA;
+        const double t0 = now_s();
+        for (int i = 0; i < c; ++i)
+            if (int r = qvti_step(sims[i], probe_steps)) return r;
+        if (cudaDeviceSynchronize() != cudaSuccess) return QVTI_ERR_CUDA;
+        *rate = (double)c * ntp * probe_steps / (now_s() - t0) / 1e9;
+        return QVTI_OK;
+    };
     double best = -1;
-    int ba = 1, bb = nkz;
+    int ba = 1, bb = nkz, bf = QVTI_FORM_PLAIN;
+    // 1. the form, one shot in flight, all kz planes at once
+    double r_plain = 0, r_tc = 0;
+    rc = probe(1, nkz, QVTI_FORM_PLAIN, &r_plain);
+    if (!rc && qvti_set_form(sims[0], QVTI_FORM_TC) == QVTI_OK) {
+        rc = probe(1, nkz, QVTI_FORM_TC, &r_tc);
+        if (!rc && r_tc > r_plain * 1.02) bf = QVTI_FORM_TC;
+    }
+    // 2. shots in flight and kz batching in that form
+    const int kzb[2] = {nkz, (nkz + 1) / 2};
     for (int b : kzb) {
-        for (int c = 1; c <= (int)sims.size(); ++c) {
-            for (int i = 0; i < c; ++i) {
-                qvti_set_kz_batch(sims[i], b);
-                qvti_reset(sims[i]);
-                qvti_step(sims[i], warm);
-            }
-            cudaDeviceSynchronize();
-            const double t0 = now_s();
-            for (int i = 0; i < c; ++i) qvti_step(sims[i], probe_steps);
-            if (cudaDeviceSynchronize() != cudaSuccess) { rc = QVTI_ERR_CUDA; break; }
-            const double rate = (double)c * ntp * probe_steps / (now_s() - t0) / 1e9;
+        for (int c = 1; c <= (int)sims.size() && rc == QVTI_OK; ++c) {
+            double rate = 0;
+            if ((rc = probe(c, b, bf, &rate))) break;
             if (rate > best * 1.02) {  // prefer fewer shots in flight unless clearly faster
                 best = rate;
                 ba = c;
                 bb = b;
             }
         }
-        if (b == kzb[1] || kzb[0] == kzb[1]) break;
+        if (rc || b == kzb[1] || kzb[0] == kzb[1]) break;
     }
     for (qvti_sim* s : sims) qvti_destroy(s);
     if (rc) return rc;
-    *best_active = ba;
-    *best_kz_batch = bb;
-    *gcell_steps = best;
+    best_out->active = ba;
+    best_out->kz_batch = bb;
+    best_out->form = bf;
+    best_out->gcell_steps = best;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[{cfg->ntx, cfg->nty, cfg->ntz, cfg->vti}] = {ba, bb};
+    g_tune[{cfg->ntx, cfg->nty, cfg->ntz, cfg->vti}] = {ba, bb, bf};
+    return QVTI_OK;
+}
+
+extern "C" int qvti_autotune(const qvti_config* cfg, int max_active, int probe_steps, int* best_active,
+                             int* best_kz_batch, double* gcell_steps)
+{
+    if (!best_active || !best_kz_batch || !gcell_steps) return QVTI_ERR_ARG;
+    qvti_tuning t{};
+    const int rc = qvti_autotune_ex(cfg, max_active, probe_steps, &t);
+    if (rc) return rc;
+    *best_active = t.active;
+    *best_kz_batch = t.kz_batch;
+    *gcell_steps = t.gcell_steps;
     return QVTI_OK;
 }

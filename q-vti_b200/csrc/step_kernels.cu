@@ -453,18 +453,6 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
         const int o0 = REGRP ? 9 * grp : grp == 0 ? 0 : 9 + (grp - 1) * 6;
         const int npen = NF * Qp;
         prefetch_group(grp + 1);
-        if (k.sigma_pf && grp + 1 < NGRP) {
-            // the next group's half spectra into L2: one 8 P-byte run (the
-            // tile's P rows) per field and kz, spread over the threads
-            const int nf1 = (REGRP || grp + 1 == 0) ? 9 : 6;
-            const int o1 = REGRP ? 9 * (grp + 1) : 9 + grp * 6;
-            const int nkz = n / 2 + 1;
-            for (int idx = threadIdx.x; idx < nf1 * nkz; idx += blockDim.x) {
-                const int f = idx / nkz, kz = idx - f * nkz;
-                const float2* a = s_src[o1 + f] + spec(k, kz, x, y0);
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
-            }
-        }
         // 1. batched C2R along z: pencil p' = f*Qp + q holds rows (2q, 2q+1)
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).

@@ -56,6 +56,11 @@ class ShotResult(ctypes.Structure):
                 ("device_ms", ctypes.c_float)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("active", ctypes.c_int), ("kz_batch", ctypes.c_int), ("form", ctypes.c_int),
+                ("gcell_steps", ctypes.c_double)]
+
+
 class RtmOpts(ctypes.Structure):
     _fields_ = [("media", ctypes.c_int), ("snap_every", ctypes.c_int), ("illum_eps", ctypes.c_float)]
 
@@ -126,6 +131,8 @@ def lib():
             "qvti_run_batch": (ctypes.c_int, [ctypes.POINTER(Shot), ctypes.c_int, ctypes.POINTER(SchedOpts),
                                               ctypes.POINTER(ShotResult), _D]),
             "qvti_autotune": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_int, _I, _I, _D]),
+            "qvti_autotune_ex": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(Tuning)]),
             "qvti_last_error": (ctypes.c_int, []),
             "qvti_error_string": (ctypes.c_char_p, [ctypes.c_int]),
         }
@@ -448,11 +455,11 @@ def run_batch(requests, max_active=0, mem_budget=0, device=0):
 
 
 def autotune(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, vti=False, max_active=4, probe_steps=8, device=0):
+    """qvti_autotune_ex: (shots in flight, kz batch, form, Gcell-steps/s)."""
     cfg = Config(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, 1 if vti else 0, device, 0.0)
-    a, b, g = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0)
-    _check(lib().qvti_autotune(ctypes.byref(cfg), max_active, probe_steps, ctypes.byref(a), ctypes.byref(b),
-                               ctypes.byref(g)), "qvti_autotune")
-    return a.value, b.value, g.value
+    t = Tuning()
+    _check(lib().qvti_autotune_ex(ctypes.byref(cfg), max_active, probe_steps, ctypes.byref(t)), "qvti_autotune_ex")
+    return t.active, t.kz_batch, t.form, t.gcell_steps
 
 
 class Server:
