@@ -232,6 +232,14 @@ int qvti_set_kz_batch(qvti_sim* sim, int kz_batch);
 enum { QVTI_FORM_PLAIN = 0, QVTI_FORM_TC = 1 };
 int qvti_set_form(qvti_sim* sim, int form);
 
+/* Failure-path check of the device-side bounded waits: queue on the
+ * simulation's stream a wait (0 < seconds <= 2) on a barrier nothing
+ * completes; when it runs out it records QVTI_ERR_TIMEOUT in the same device
+ * flag a stalled tensor-core round would, so the next qvti_sync returns
+ * QVTI_ERR_TIMEOUT; qvti_reset clears it and the simulation stays usable.
+ * No counterpart in the reference. */
+int qvti_probe_bounded_wait(qvti_sim* sim, double seconds);
+
 /* ---------------------------------------------------------------------
  * Reverse-time migration and Q compensation.  The reference declares these
  * as flags only (viscoelas_3D.cpp:1-3 "viscoacoustic reverse time

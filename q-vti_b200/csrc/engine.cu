@@ -1063,6 +1063,18 @@ extern "C" int qvti_set_form(qvti_sim* s, int form)
     return QVTI_OK;
 }
 
+extern "C" int qvti_probe_bounded_wait(qvti_sim* s, double seconds)
+{
+    using namespace qvti;
+    if (!s || !(seconds > 0.0 && seconds <= 2.0)) return fail(QVTI_ERR_ARG);
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    int clock_khz = 0;
+    QV_CUDA(cudaDeviceGetAttribute(&clock_khz, cudaDevAttrClockRate, s->cfg.device));
+    launch_wait_probe(s->d_err, (long long)(seconds * 1e3 * clock_khz), s->st);
+    QV_CUDA(cudaGetLastError());
+    return QVTI_OK;
+}
+
 extern "C" int qvti_last_error(void) { return qvti::g_last_error; }
 
 extern "C" const char* qvti_error_string(int code)

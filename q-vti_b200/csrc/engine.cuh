@@ -46,16 +46,6 @@ constexpr int kNumG = 27;
 constexpr int kNumGxy = kNumG - 6;  // fields that go through k_mx and k_cy
 __host__ __device__ constexpr bool is_gz(int o) { return o == 7 || o == 10 || o == 22; }
 __host__ __device__ constexpr bool is_gy(int o) { return o == 4 || o == 16 || o == 25; }
-// G index of the c-th field that goes through the x and y passes.
-__host__ __device__ inline int gxy_field(int c)
-{
-    int o = -1;
-    for (int n = 0; n <= c;) {
-        ++o;
-        if (!is_gz(o) && !is_gy(o)) ++n;
-    }
-    return o;
-}
 
 struct KP {
     int nx, ny, nz, nkz, pml;
@@ -182,6 +172,8 @@ bool tc_cy_available(const KP& k);
 size_t tc_cy_smem();
 int configure_tc_kernels();
 void launch_dft16_tables(float* out, cudaStream_t st);  // 4096 floats
+// A bounded wait that runs out after limit_cycles and records QVTI_ERR_TIMEOUT in *err.
+void launch_wait_probe(int* err, long long limit_cycles, cudaStream_t st);
 void launch_cy_tc(const KP& k, bool inv, int nfield, long long line0, long long line_end, cudaStream_t st);
 
 // Individual stages, exposed for unit tests through the C ABI.

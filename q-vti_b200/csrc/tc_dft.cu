@@ -41,6 +41,21 @@ constexpr int kTcLines = 8;
 constexpr int kTcN = 256;        // transform length of this form
 constexpr uint32_t kTmemCols = 32;
 
+// G index of each of the 21 fields of the x and y passes (all but the
+// one-axis fields, is_gz / is_gy), the order k_cy's inverse pass uses.
+struct GxyTable {
+    int v[kNumGxy];
+};
+constexpr GxyTable make_gxy()
+{
+    GxyTable t{};
+    int n = 0;
+    for (int o = 0; o < kNumG; ++o)
+        if (!is_gz(o) && !is_gy(o)) t.v[n++] = o;
+    return t;
+}
+__constant__ GxyTable c_gxy_tc = make_gxy();
+
 // ------------------------------------------------------------ PTX wrappers --
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -101,12 +116,13 @@ __device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity)
     return ok != 0;
 }
 
-// Wait for an MMA round, at most ~2 s of SM clock; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity)
+// Wait for an mbarrier phase, at most `limit` SM clock cycles (default ~2 s
+// at the B200's 1.97 GHz, for an MMA round); false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = 4000000000ll)
 {
     const long long t0 = clock64();
     while (!mbar_try(mbar, parity))
-        if (clock64() - t0 > 4000000000ll) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -251,35 +267,38 @@ __global__ void __launch_bounds__(kTcThreads, INV ? 5 : 4) k_cy_tc(KP k, int nfi
     uint32_t phase = 0;
     bool ok = true;
 
-    const long long nlines = line_end - line0;
-    const long long ntile = (nlines + kTcLines - 1) / kTcLines;
-    const long long total = ntile * nfield;
+    // tile counts fit 32 bits (at most 21 fields x (nz/2+1) nx / 8 tiles);
+    // only the element offsets need 64
+    const int nlines = (int)(line_end - line0);
+    const int ntile = (nlines + kTcLines - 1) / kTcLines;
+    const int total = ntile * nfield;
     const float inv_n = 1.0f / ((float)kTcN * (float)k.nz);
     const float* Bhi = INV ? Bi_hi : Bf_hi;
     const float* Blo = INV ? Bi_lo : Bf_lo;
     // tile w: field c, lines [first, first + lv)
-    auto tile = [&](long long w, int& c, long long& first, int& lv) {
-        c = (int)(w / ntile);
-        first = line0 + (w - (long long)c * ntile) * kTcLines;
-        lv = (int)min((long long)kTcLines, line_end - first);
+    auto tile = [&](int w, int& c, long long& first, int& lv) {
+        c = w / ntile;
+        const int t = (w - c * ntile) * kTcLines;
+        first = line0 + t;
+        lv = min(kTcLines, nlines - t);
     };
     // stage 0 inputs of butterfly j of line p: x[j + 16 r]
     auto load = [&](int c, long long first, int lv, float2* v) {
-        const float2* src = (INV ? k.G[gxy_field(c)] : k.H[c]) + first * kTcN;
+        const float2* src = (INV ? k.G[c_gxy_tc.v[c]] : k.H[c]) + first * kTcN;
 #pragma unroll
         for (int r = 0; r < 16; ++r) v[r] = p < lv ? src[(long long)p * kTcN + j + 16 * r] : make_float2(0.f, 0.f);
     };
     int c, lv, shift_c = -1;  // shift_c: field whose shift table is in tsh
     long long first;
     float2 v[16];
-    long long w = blockIdx.x;
+    int w = blockIdx.x;
     if (w < total) {
         tile(w, c, first, lv);
         load(c, first, lv, v);
     }
     for (; ok && w < total; w += gridDim.x) {
         const long long off = first * kTcN;
-        float2* dst = (INV ? k.G[gxy_field(c)] : k.Hy[c]) + off;
+        float2* dst = (INV ? k.G[c_gxy_tc.v[c]] : k.Hy[c]) + off;
         float2* ydst = (!INV && k.Yv[c]) ? k.Yv[c] + off : nullptr;
         if (ydst && shift_c != c) {
             // all threads are past the previous tile's reads of tsh (the
@@ -291,7 +310,7 @@ __global__ void __launch_bounds__(kTcThreads, INV ? 5 : 4) k_cy_tc(KP k, int nfi
         put_row(Ahi, Alo, t, v);
         // the next tile's inputs, in flight during this tile's rounds
         const int c_cur = c, lv_cur = lv;
-        const long long wn = w + gridDim.x;
+        const int wn = w + gridDim.x;
         if (wn < total) {
             tile(wn, c, first, lv);
             load(c, first, lv, v);
@@ -342,6 +361,19 @@ __global__ void __launch_bounds__(kTcThreads, INV ? 5 : 4) k_cy_tc(KP k, int nfi
     if (t < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
+// The timeout path of the bounded waits, exercised without a fault: one
+// thread waits, at most `limit` cycles, on an mbarrier phase that nothing
+// completes, then records QVTI_ERR_TIMEOUT in the engine's device error flag
+// exactly as a stalled MMA round would.
+__global__ void k_wait_probe(int* err, long long limit)
+{
+    __shared__ uint64_t bar;
+    const uint32_t mbar = smem_u32(&bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!mbar_wait(mbar, 0, limit) && err) atomicExch(err, QVTI_ERR_TIMEOUT);
+}
+
 // 16-point DFT matrices for the MMA's B operand (N = 32 outputs x K = 32
 // inputs, both as interleaved re/im), FP64-built and split into TF32 hi and
 // lo parts, stored in the swizzled K-major layout the kernel copies as is:
@@ -384,6 +416,11 @@ int configure_tc_kernels()
 }
 
 void launch_dft16_tables(float* out, cudaStream_t st) { k_dft16_tables<<<16, 128, 0, st>>>(out); }
+
+void launch_wait_probe(int* err, long long limit_cycles, cudaStream_t st)
+{
+    k_wait_probe<<<1, 1, 0, st>>>(err, limit_cycles);
+}
 
 void launch_cy_tc(const KP& k, bool inv, int nfield, long long line0, long long line_end, cudaStream_t st)
 {

@@ -118,6 +118,7 @@ def lib():
             "qvti_set_kz_batch": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_set_form": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_set_media": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_probe_bounded_wait": (ctypes.c_int, [_V, ctypes.c_double]),
             "qvti_set_injection": (ctypes.c_int, [_V, _F, _F, _F, ctypes.c_int]),
             "qvti_rtm_shot": (ctypes.c_int, [ctypes.POINTER(Config), _F, _F, _F, _F, _F, _F, _F, ctypes.c_int,
                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, ctypes.c_int,

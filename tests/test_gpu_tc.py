@@ -50,3 +50,26 @@ def test_tc_form_needs_a_256_point_y_axis(qvti):
         sim.set_form(qvti.FORM_TC)
         with pytest.raises(qvti.QvtiError, match="invalid argument"):
             sim.set_form(7)
+
+
+def test_bounded_wait_reports_a_timeout_and_the_simulation_recovers(qvti):
+    """The tensor-core rounds wait on an mbarrier with a time limit; when it
+    runs out the kernel records QVTI_ERR_TIMEOUT in the engine's device flag
+    and returns.  Exercised without a fault: a 50 ms wait on a barrier that
+    nothing completes.  qvti_sync reports the timeout; after qvti_reset the
+    simulation steps and records as before."""
+    c = _ct_case((16, 256, 24), 40, pml=4)
+    ref = qvti.run_case(c, vti=True, form=qvti.FORM_TC)["rec"]
+    with qvti.simulation_for_case(c, vti=True) as sim:
+        sim.set_form(qvti.FORM_TC)
+        sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"], c["eps"], c["delta"])
+        sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])
+        sim.set_source(c["s_ix"], c["s_iy"], int(c["s_iz"]) + 10, np.asarray(c["rik"], np.float32))
+        sim.reset()
+        qvti._check(qvti.lib().qvti_probe_bounded_wait(sim._h, 0.05), "qvti_probe_bounded_wait")
+        with pytest.raises(qvti.QvtiError, match="timed out"):
+            sim.sync()
+        sim.reset()
+        sim.step(40)
+        sim.sync()
+        assert np.array_equal(sim.records(), ref)
