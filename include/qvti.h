@@ -232,6 +232,33 @@ int qvti_set_kz_batch(qvti_sim* sim, int kz_batch);
 enum { QVTI_FORM_PLAIN = 0, QVTI_FORM_TC = 1 };
 int qvti_set_form(qvti_sim* sim, int form);
 
+/* Tile of each step kernel, in the order QVTI_TILE_*: the z rows of a k_vy
+ * or k_vx block, the y rows of a k_fz, k_mx or k_sigma block, the lines of
+ * a k_cy block.  tiles[i] = 0 keeps kernel i's default (its compiled
+ * kernel's tile where the transform length has one); tiles[i] > 0 runs the
+ * runtime-length kernel with that tile: even, 2..32, dividing the axis it
+ * tiles (k_cy: any), and the step's shared memory within the device limit,
+ * else QVTI_ERR_UNSUPPORTED and the tiling is unchanged.  The results agree
+ * with the default tiling to FP32 rounding.  A tuning knob of
+ * qvti_autotune_tiles; no counterpart in the reference. */
+enum { QVTI_TILE_VY = 0, QVTI_TILE_VX, QVTI_TILE_FZ, QVTI_TILE_CY, QVTI_TILE_MX, QVTI_TILE_SIGMA, QVTI_NUM_TILES };
+int qvti_set_tiles(qvti_sim* sim, const int tiles[QVTI_NUM_TILES]);
+/* The tiles the step launches take and, per kernel, 1 where it runs its
+ * runtime-length kernel (either may be null). */
+int qvti_get_tiles(qvti_sim* sim, int tiles[QVTI_NUM_TILES], int runtime[QVTI_NUM_TILES]);
+
+/* Per-kernel tile search on a simulation whose model and source are set:
+ * for each step kernel, its default and the runtime-length kernel at every
+ * valid tile in {2, 4, 8, 16, 32}, each timed over probe_steps profiled
+ * steps (CUDA events between the kernels) after a reset and one warm-up
+ * step, the kernels already searched at their chosen tiles, the rest at
+ * their defaults; a tile other than the default is taken only when it is at
+ * least 3 % faster.  Leaves the chosen tiling set and the simulation reset.
+ * best[i]: the chosen setting (0 = default), ms[i]: its time (either may be
+ * null).  Needs nt >= probe_steps + 1 steps of wavelet capacity.  No
+ * counterpart in the reference. */
+int qvti_autotune_tiles(qvti_sim* sim, int probe_steps, int best[QVTI_NUM_TILES], float ms[QVTI_NUM_TILES]);
+
 /* Failure-path check of the device-side bounded waits: queue on the
  * simulation's stream a wait (0 < seconds <= 2) on a barrier nothing
  * completes; when it runs out it records QVTI_ERR_TIMEOUT in the same device
@@ -352,17 +379,19 @@ int qvti_run_batch(const qvti_shot* shots, int n, const qvti_sched_opts* opts, q
                    double* wall_s);
 
 /* Probe one grid: the form of the transforms (plain FP32 stages, or the
- * tensor-core DFT plan where the grid has one) with one shot in flight, then
- * probe_steps steps on 1..max_active concurrent simulations (homogeneous
- * model) for each kz batch in {nz/2+1, (nz/2+2)/2}; report the fastest
- * setting and its Gcell-steps/s.  The scheduler caches the result per grid
- * and applies it to the shots of that grid.  No counterpart in the
- * reference, which runs one shot at a time (viscoelas_3D.cpp:355-405). */
+ * tensor-core DFT plan where the grid has one) with one shot in flight, the
+ * per-kernel tiles in that form (qvti_autotune_tiles), then probe_steps
+ * steps on 1..max_active concurrent simulations (homogeneous model) for
+ * each kz batch in {nz/2+1, (nz/2+2)/2}; report the fastest setting and its
+ * Gcell-steps/s.  The scheduler caches the result per grid and applies it
+ * to the shots of that grid.  No counterpart in the reference, which runs
+ * one shot at a time (viscoelas_3D.cpp:355-405). */
 typedef struct {
     int active;          /* shots in flight                                   */
     int kz_batch;        /* kz planes per batch of the k-space passes         */
     int form;            /* QVTI_FORM_PLAIN or QVTI_FORM_TC                   */
     double gcell_steps;  /* measured Gcell-steps/s of that setting            */
+    int tiles[QVTI_NUM_TILES]; /* per-kernel tiles (qvti_set_tiles)           */
 } qvti_tuning;
 int qvti_autotune_ex(const qvti_config* cfg, int max_active, int probe_steps, qvti_tuning* best);
 

@@ -203,8 +203,17 @@ struct Sim {
     int nt = 0, rn = 0;
     bool have_model = false, have_src = false;
     int steps = 0;
-    cudaGraphExec_t gexec = nullptr;
+    // the step loop as CUDA graphs: one step, and kGraphSteps steps (built
+    // when a call first asks for that many); both rebuilt after any change
+    // to the launch parameters
+    cudaGraphExec_t gexec = nullptr, gexec_n = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void drop_graphs()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (gexec_n) cudaGraphExecDestroy(gexec_n);
+        gexec = gexec_n = nullptr;
+    }
 
     // Device arrays come from the stream-ordered allocator on the
     // simulation's own stream: creating or freeing a simulation then orders
@@ -238,7 +247,7 @@ struct Sim {
     }
     ~Sim()
     {
-        if (gexec) cudaGraphExecDestroy(gexec);
+        drop_graphs();
         for (void* p : allocs)
             if (p) cudaFreeAsync(p, st);
         if (st) cudaStreamSynchronize(st);
@@ -283,18 +292,25 @@ int slab_arrays(const KP& k, float** out, size_t* len)
 }
 constexpr int kNumSlab = 9 + 8 + 8 + 6 + 6;
 
-int build_graph(Sim* s)
+// Steps per multi-step graph: 16 steps are 128 kernel nodes, and a chunk of
+// the scheduler (32 steps) is two launches.
+constexpr int kGraphSteps = 16;
+
+// Captures `nsteps` steps into *out (the step counter lives on the device,
+// so every replay advances it).
+int build_graph(Sim* s, int nsteps, cudaGraphExec_t* out)
 {
-    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    if (*out) { cudaGraphExecDestroy(*out); *out = nullptr; }
     cudaGraph_t g = nullptr;
     QV_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-    launch_step(s->kp, s->st);
+    for (int i = 0; i < nsteps; ++i) launch_step(s->kp, s->st);
     QV_CUDA(cudaStreamEndCapture(s->st, &g));
-    cudaError_t e = cudaGraphInstantiate(&s->gexec, g, 0);
+    cudaError_t e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     QV_CUDA(e);
     return QVTI_OK;
 }
+int build_graph(Sim* s) { return build_graph(s, 1, &s->gexec); }
 
 }  // namespace
 }  // namespace qvti
@@ -417,6 +433,7 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.err = s->d_err;
     k.form = kFormPlain;
     k.loss_scale = 1.0f;
+    k.hz_scale = 1;
     k.inj[0] = k.inj[1] = k.inj[2] = nullptr;
     k.inj_nt = 0;
 
@@ -539,7 +556,7 @@ extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_
         s->rec_cap = cap;
     }
     s->have_src = true;
-    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    s->drop_graphs();
     return QVTI_OK;
 }
 
@@ -577,7 +594,7 @@ extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const 
         }
         s->rec_cap = cap;
     }
-    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    s->drop_graphs();
     return QVTI_OK;
 }
 
@@ -614,11 +631,19 @@ extern "C" int qvti_step(qvti_sim* s, int nsteps)
     if (!s->have_model || !s->have_src) return fail(QVTI_ERR_STATE);
     if (s->steps + nsteps > s->nt) return fail(QVTI_ERR_ARG);  // wavelet / record capacity
     QV_CUDA(cudaSetDevice(s->cfg.device));
-    if (!s->gexec) {
+    int left = nsteps;
+    if (left >= kGraphSteps) {
+        if (!s->gexec_n) {
+            int rc = build_graph(s, kGraphSteps, &s->gexec_n);
+            if (rc) return rc;
+        }
+        for (; left >= kGraphSteps; left -= kGraphSteps) QV_CUDA(cudaGraphLaunch(s->gexec_n, s->st));
+    }
+    if (left > 0 && !s->gexec) {
         int rc = build_graph(s);
         if (rc) return rc;
     }
-    for (int i = 0; i < nsteps; ++i) QV_CUDA(cudaGraphLaunch(s->gexec, s->st));
+    for (; left > 0; --left) QV_CUDA(cudaGraphLaunch(s->gexec, s->st));
     s->steps += nsteps;
     return QVTI_OK;
 }
@@ -628,9 +653,16 @@ extern "C" int qvti_step_timed(qvti_sim* s, int nsteps, float* ms)
     using namespace qvti;
     if (!s || !ms) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
-    if (!s->gexec && s->have_model && s->have_src) {
-        int rc = build_graph(s);
-        if (rc) return rc;
+    // both graphs the call replays are built before the first event
+    if (s->have_model && s->have_src) {
+        if (!s->gexec) {
+            int rc = build_graph(s);
+            if (rc) return rc;
+        }
+        if (nsteps >= kGraphSteps && !s->gexec_n) {
+            int rc = build_graph(s, kGraphSteps, &s->gexec_n);
+            if (rc) return rc;
+        }
     }
     QV_CUDA(cudaStreamSynchronize(s->st));
     QV_CUDA(cudaEventRecord(s->ev0, s->st));
@@ -1005,7 +1037,7 @@ extern "C" int qvti_set_kz_batch(qvti_sim* s, int kz_batch)
     if (!s || kz_batch < 1 || kz_batch > s->nkz) return fail(QVTI_ERR_ARG);
     if (s->kp.kz_batch != kz_batch) {
         s->kp.kz_batch = kz_batch;
-        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        s->drop_graphs();
     }
     return QVTI_OK;
 }
@@ -1018,7 +1050,7 @@ extern "C" int qvti_set_media(qvti_sim* s, int media)
     const float ls = media == QVTI_MEDIA_VISCOELASTIC ? 1.0f : media == QVTI_MEDIA_Q_COMPENSATED ? -1.0f : 0.0f;
     if (s->kp.loss_scale != ls) {
         s->kp.loss_scale = ls;
-        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        s->drop_graphs();
     }
     // the lossless medium's coefficients are built without gamma: a model
     // set before this call is out of date
@@ -1045,7 +1077,7 @@ extern "C" int qvti_set_injection(qvti_sim* s, const float* vx, const float* vy,
     }
     k.inj_nt = nt;
     QV_CUDA(cudaStreamSynchronize(s->st));
-    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    s->drop_graphs();
     return QVTI_OK;
 }
 
@@ -1058,7 +1090,101 @@ extern "C" int qvti_set_form(qvti_sim* s, int form)
     if (form == QVTI_FORM_TC && !tc_cy_available(probe)) return fail(QVTI_ERR_UNSUPPORTED);
     if (s->kp.form != probe.form) {
         s->kp.form = probe.form;
-        if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+        s->drop_graphs();
+    }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_set_tiles(qvti_sim* s, const int tiles[QVTI_NUM_TILES])
+{
+    using namespace qvti;
+    static_assert(QVTI_NUM_TILES == kNumTiled, "one tile per step kernel");
+    if (!s || !tiles) return fail(QVTI_ERR_ARG);
+    KP probe = s->kp;
+    bool same = true;
+    for (int i = 0; i < kNumTiled; ++i) {
+        probe.tile_rt[i] = tiles[i];
+        same = same && tiles[i] == s->kp.tile_rt[i];
+    }
+    if (!tiles_valid(probe)) return fail(QVTI_ERR_UNSUPPORTED);
+    if (!same) {
+        s->kp = probe;
+        s->drop_graphs();
+    }
+    return QVTI_OK;
+}
+
+extern "C" int qvti_get_tiles(qvti_sim* s, int tiles[QVTI_NUM_TILES], int runtime[QVTI_NUM_TILES])
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    step_tile_set(s->kp, tiles, runtime);
+    return QVTI_OK;
+}
+
+extern "C" int qvti_autotune_tiles(qvti_sim* s, int probe_steps, int best[QVTI_NUM_TILES], float ms_out[QVTI_NUM_TILES])
+{
+    using namespace qvti;
+    if (!s || probe_steps < 1) return fail(QVTI_ERR_ARG);
+    if (!s->have_model || !s->have_src) return fail(QVTI_ERR_STATE);
+    if (s->nt < probe_steps + 1) return fail(QVTI_ERR_ARG);
+    // the step kernels' profile slots each tile setting times: k_vy, k_vx,
+    // k_fz, k_cy (forward + inverse), k_mx, k_sigma
+    auto kernel_ms = [](int i, const float* ms) {
+        switch (i) {
+            case 0: return ms[0];
+            case 1: return ms[1];
+            case 2: return ms[2];
+            case 3: return ms[3] + ms[5];
+            case 4: return ms[4];
+            default: return ms[6];
+        }
+    };
+    int chosen[kNumTiled] = {};
+    float chosen_ms[kNumTiled] = {};
+    auto time_of = [&](int i, const int* tiles, float* t) -> int {
+        float ms[kStepKernels];
+        int rc;
+        if ((rc = qvti_set_tiles(s, tiles)) || (rc = qvti_reset(s)) ||
+            (rc = qvti_profile_step(s, 1, kStepKernels, nullptr, nullptr, ms, nullptr)) ||
+            (rc = qvti_profile_step(s, probe_steps, kStepKernels, nullptr, nullptr, ms, nullptr)))
+            return rc;
+        *t = kernel_ms(i, ms);
+        return QVTI_OK;
+    };
+    int saved[kNumTiled];
+    std::memcpy(saved, s->kp.tile_rt, sizeof saved);
+    int rc = QVTI_OK;
+    for (int i = 0; i < kNumTiled && rc == QVTI_OK; ++i) {
+        int cand[kNumTiled];
+        std::memcpy(cand, chosen, sizeof cand);
+        cand[i] = 0;
+        float t_def = 0.f;
+        if ((rc = time_of(i, cand, &t_def))) break;
+        float t_best = t_def;
+        for (int t : {2, 4, 8, 16, 32}) {
+            cand[i] = t;
+            KP probe = s->kp;
+            std::memcpy(probe.tile_rt, cand, sizeof cand);
+            if (!tiles_valid(probe)) continue;
+            float tt = 0.f;
+            if ((rc = time_of(i, cand, &tt))) break;
+            if (tt < 0.97f * t_def && tt < t_best) {
+                t_best = tt;
+                chosen[i] = t;
+            }
+        }
+        chosen_ms[i] = t_best;
+    }
+    if (rc) {
+        qvti_set_tiles(s, saved);
+        qvti_reset(s);
+        return rc;
+    }
+    if ((rc = qvti_set_tiles(s, chosen)) || (rc = qvti_reset(s))) return rc;
+    for (int i = 0; i < kNumTiled; ++i) {
+        if (best) best[i] = chosen[i];
+        if (ms_out) ms_out[i] = chosen_ms[i];
     }
     return QVTI_OK;
 }

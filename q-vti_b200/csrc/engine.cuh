@@ -103,8 +103,19 @@ struct KP {
     // none), the adjoint source of back-propagation
     const float* inj[3];
     int inj_nt;
+    // tile of each step kernel (k_vy, k_vx, k_fz, k_cy, k_mx, k_sigma):
+    // 0 = the default (the compiled kernel's tile, or the runtime kernel's
+    // where the length has no compiled kernel); > 0 = the runtime kernel
+    // with this tile (qvti_set_tiles, checked by tiles_valid)
+    int tile_rt[6];
+    // 1: k_cy's forward pass leaves H[c] multiplied by the z shift
+    // multiplier of c's kz-only field over nz (Fz for vz, Bz for vx and vy),
+    // which is what k_sigma's C2R of that field reads; 0: H is left as k_fz
+    // wrote it (the standalone stage entry points)
+    int hz_scale;
 };
 constexpr int kFormPlain = 0, kFormTc = 1;
+constexpr int kNumTiled = 6;
 
 // C-PML memory variables are non-zero only inside their axis' slabs (b = 0
 // elsewhere, cuviscoelas_3D.cu:291-307), so each is stored for the 2 pml
@@ -148,6 +159,13 @@ struct StepProfile {
 void launch_step(const KP& kp, cudaStream_t st, StepProfile* prof = nullptr);
 // Largest dynamic shared memory (bytes) one of the step's launches needs.
 size_t step_smem_bytes(const KP& kp);
+// Tiles the step's launches take (tile_rt applied); runtime[i]: kernel i
+// takes its runtime-length path.
+void step_tile_set(const KP& kp, int tiles[kNumTiled], int runtime[kNumTiled]);
+// Whether kp.tile_rt is a tiling the kernels support for this grid: every
+// tile even, at most 32, dividing the axis it tiles (k_cy: any line
+// count), and the step's shared memory within kMaxSmem.
+bool tiles_valid(const KP& kp);
 constexpr size_t kMaxSmem = 226 * 1024;  // dynamic; an SM block takes 227 KB with static
 // coef_out: 7 model arrays (rho gp gs c11 c33 c13 cs) then the 5 S-set arrays
 // (input of the MU average).

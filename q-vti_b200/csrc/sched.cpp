@@ -7,7 +7,8 @@
 // flight on one GPU at once:
 //
 //   * every shot runs on a pooled simulation (one stream each) whose time
-//     loop is a CUDA graph of one step, launched in chunks of kChunk steps
+//     loop is CUDA graphs of 16 steps (and of one step for a remainder),
+//     launched in chunks of kChunk steps
 //     with at most two chunks queued ahead, so a long shot never fills the
 //     launch queue and the scheduler thread stays free;
 //   * shots are admitted first in, first out when a slot and device memory
@@ -70,6 +71,7 @@ struct ShapeKey {
 
 struct Tuning {
     int active, kz_batch, form;
+    int tiles[QVTI_NUM_TILES];
 };
 std::mutex g_tune_mu;
 std::map<ShapeKey, Tuning> g_tune;
@@ -250,6 +252,7 @@ int qvti_server::start(Job* j, PoolSim* ps)
     if (cached_tuning({s.ntx, s.nty, s.ntz, s.vti}, &t)) {
         if ((rc = qvti_set_kz_batch(sim, t.kz_batch))) return rc;
         if ((rc = qvti_set_form(sim, t.form))) return rc;
+        if ((rc = qvti_set_tiles(sim, t.tiles))) return rc;
     }
     if ((rc = qvti_set_model(sim, s.velp, s.vels, s.rho, s.gama_p, s.gama_s, s.eps, s.delta, 0))) return rc;
     if ((rc = qvti_set_receivers(sim, s.r_iz, s.r_ix, s.r_iy, s.rn))) return rc;
@@ -571,6 +574,7 @@ extern "C" int qvti_autotune_ex(const qvti_config* cfg, int max_active, int prob
     };
     double best = -1;
     int ba = 1, bb = nkz, bf = QVTI_FORM_PLAIN;
+    int tiles[QVTI_NUM_TILES] = {};
     // 1. the form, one shot in flight, all kz planes at once
     double r_plain = 0, r_tc = 0;
     rc = probe(1, nkz, QVTI_FORM_PLAIN, &r_plain);
@@ -578,7 +582,11 @@ extern "C" int qvti_autotune_ex(const qvti_config* cfg, int max_active, int prob
         rc = probe(1, nkz, QVTI_FORM_TC, &r_tc);
         if (!rc && r_tc > r_plain * 1.02) bf = QVTI_FORM_TC;
     }
-    // 2. shots in flight and kz batching in that form
+    // 2. per-kernel tiles in that form, applied to every probe simulation
+    if (!rc && !(rc = qvti_set_form(sims[0], bf)) && !(rc = qvti_set_kz_batch(sims[0], nkz)))
+        rc = qvti_autotune_tiles(sims[0], probe_steps, tiles, nullptr);
+    for (size_t i = 0; i < sims.size() && rc == QVTI_OK; ++i) rc = qvti_set_tiles(sims[i], tiles);
+    // 3. shots in flight and kz batching in that form
     const int kzb[2] = {nkz, (nkz + 1) / 2};
     for (int b : kzb) {
         for (int c = 1; c <= (int)sims.size() && rc == QVTI_OK; ++c) {
@@ -598,8 +606,10 @@ extern "C" int qvti_autotune_ex(const qvti_config* cfg, int max_active, int prob
     best_out->kz_batch = bb;
     best_out->form = bf;
     best_out->gcell_steps = best;
+    Tuning t{ba, bb, bf, {}};
+    for (int i = 0; i < QVTI_NUM_TILES; ++i) best_out->tiles[i] = t.tiles[i] = tiles[i];
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[{cfg->ntx, cfg->nty, cfg->ntz, cfg->vti}] = {ba, bb, bf};
+    g_tune[{cfg->ntx, cfg->nty, cfg->ntz, cfg->vti}] = t;
     return QVTI_OK;
 }
 

@@ -125,7 +125,10 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
 // reads or writes 16 consecutive points (128 bytes) of one line, so a warp
 // access touches two lines, and the radix-16 shared-memory stages are
 // conflict-free.  The field is H[0..2] (forward) or G[0..26] (inverse), by
-// blockIdx.y.
+// blockIdx.y.  The forward pass (KP::hz_scale) also leaves each H value it
+// reads multiplied by M(kz) / nz, M the z shift multiplier of the
+// component's kz-only field (Fz for vz, Bz for vx and vy): k_sigma then
+// inverse-transforms that field straight from H.
 constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
 
 template <int N, bool INV>
@@ -139,18 +142,31 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     float2* A = tw + n;
     float2* B = A + L * (n + n / 16);
     float2* C = B + L * (n + n / 16);  // forward with Yv: the lines' y spectra, [L][n]
+    float2* hm = C + L * n;            // forward: M(kz) / nz of each line (hz_scale)
     load_table(tw, k.tw_y, n);
-    __syncthreads();
     // forward: H -> Hy (H stays for k_sigma's kz-only fields); inverse: G in
     // place, blockIdx.y over the fields that went through k_mx
     const int c = blockIdx.y;
     const long long first = line0 + (long long)blockIdx.x * L;
     const int lv = (int)min((long long)L, line_end - first);  // lines of the tile inside the batch
+    const bool hs = !INV && k.hz_scale;
+    if (hs) {
+        const float2* M = c == 2 ? k.Fz : k.Bz;
+        const float inv_nz = 1.0f / k.nz;
+        for (int p = threadIdx.x; p < lv; p += blockDim.x) hm[p] = cscale(M[(int)(first + p) / k.nx], inv_nz);
+    }
+    __syncthreads();
     const long long off = first * n;
     const float2* src = (INV ? k.G[c_gxy[c]] : k.H[c]) + off;
     float2* dst = (INV ? k.G[c_gxy[c]] : k.Hy[c]) + off;
+    float2* hsc = k.H[c] + off;  // hs: written where read, by the reading thread
     const bool ydv = !INV && k.Yv[c] != nullptr;
-    auto load = [&](int p, int i) -> float2 { return p < lv ? src[(long long)p * n + i] : make_float2(0.f, 0.f); };
+    auto load = [&](int p, int i) -> float2 {
+        if (p >= lv) return make_float2(0.f, 0.f);
+        const float2 v = src[(long long)p * n + i];
+        if (hs) hsc[(long long)p * n + i] = cmul(v, hm[p]);
+        return v;
+    };
     auto store = [&](int p, int i, float2 v) {
         if (p < lv) dst[(long long)p * n + i] = v;
         if (ydv) C[p * n + i] = v;
@@ -371,17 +387,14 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
     }
     const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
     // where each of the 27 fields comes from: G (x/y passes), Yv (forward y
-    // pass, already scaled) or H times the z shift multiplier (kind 1:
-    // forward, 2: backward)
+    // pass, already scaled) or H, which the forward y pass left multiplied
+    // by the z shift multiplier over nz (Fz for vz, field 7; Bz for vx and
+    // vy, fields 10 and 22)
     __shared__ const float2* s_src[kNumG];
-    __shared__ int s_kind[kNumG];
-    for (int o = threadIdx.x; o < kNumG; o += blockDim.x) {
+    for (int o = threadIdx.x; o < kNumG; o += blockDim.x)
         s_src[o] = is_gz(o) ? k.H[o == 7 ? 2 : o == 10 ? 0 : 1] : is_gy(o) ? k.Yv[o == 4 ? 1 : o == 16 ? 0 : 2] : k.G[o];
-        s_kind[o] = is_gz(o) ? (o == 7 ? 1 : 2) : 0;
-    }
     __syncthreads();
     const int it = *k.d_it;
-    const float inv_nz = 1.0f / n;
     // inv_dt enters only the loss terms (the spectral time derivative of the
     // constant-Q loss operator): their sign and presence follow the medium
     // (k.loss_scale: 1 viscoelastic, 0 dispersion only, -1 Q-compensated)
@@ -457,20 +470,14 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
         // a kz-only field (is_gz) is M(kz) H(kz) / nz, a ky-only one (is_gy)
-        // Yv, which the forward y pass scaled alike: the values the x and y
-        // round trip (normalised by 1/ntp) would have produced
+        // Yv: the forward y pass left both so, the values the x and y round
+        // trip (normalised by 1/ntp) would have produced
         auto load = [&](int pp, int i) -> float2 {
             const int f = pp / Qp, q = pp - f * Qp, o = o0 + f;
             if (RAG && 2 * q >= yv) return make_float2(0.f, 0.f);
             const int kk = i <= n / 2 ? i : n - i;
             const float4 gg = *reinterpret_cast<const float4*>(s_src[o] + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
-            const int kind = s_kind[o];
-            if (kind) {
-                const float2 m = cscale(tzs[(kind == 1 ? 0 : n) + kk], inv_nz);
-                a = cmul(a, m);
-                b = cmul(b, m);
-            }
             if (kk == 0 || 2 * kk == n) { a.y = 0.f; b.y = 0.f; }
             if (i > n / 2) { a.y = -a.y; b.y = -b.y; }
             return make_float2(a.x - b.y, a.y + b.x);
@@ -1383,9 +1390,10 @@ int tile_of(int n, int want)
 }
 
 size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + k.nz / 16)); }
-size_t smem_cy(const KP& k, int L, bool ydv = false)
+// fwd: the forward pass's y-spectrum tile and per-line multipliers
+size_t smem_cy(const KP& k, int L, bool fwd = false)
 {
-    return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16) + (ydv ? (size_t)L * k.ny : 0));
+    return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16) + (fwd ? (size_t)L * k.ny + L : 0));
 }
 size_t smem_mx(const KP& k, int P)
 {
@@ -1464,20 +1472,29 @@ int cdiv(int a, int b) { return (a + b - 1) / b; }
 // takes its full tile along the other axis, the last tile ragged (its rows
 // or lines past the grid read as zeros and are not written); otherwise the
 // runtime path takes the largest power-of-two divisor of the tiled axis up
-// to the full tile.
+// to the full tile.  A tile set in KP::tile_rt selects the runtime path with
+// that tile.
 struct StepTiles {
     int vy, vx, fz, cy, mx, sigma;
+    bool rt[kNumTiled];  // runtime path, in the order above
 };
 StepTiles step_tiles(const KP& k)
 {
-    auto tile = [](int len, int tiled, int want) { return ct_length(len) ? want : tile_of(tiled, want); };
     StepTiles t;
-    t.vy = tile(k.ny, k.nz, 16);
-    t.vx = tile(k.nx, k.nz, 16);
-    t.fz = tile(k.nz, k.ny, 16);
-    t.cy = tile(k.ny, k.nx, 8);
-    t.mx = tile(k.nx, k.ny, 16);
-    t.sigma = tile(k.nz, k.ny, kSigmaRows);
+    auto tile = [&](int i, int len, int tiled, int want) {
+        if (k.tile_rt[i] > 0) {
+            t.rt[i] = true;
+            return k.tile_rt[i];
+        }
+        t.rt[i] = !ct_length(len);
+        return t.rt[i] ? tile_of(tiled, want) : want;
+    };
+    t.vy = tile(0, k.ny, k.nz, 16);
+    t.vx = tile(1, k.nx, k.nz, 16);
+    t.fz = tile(2, k.nz, k.ny, 16);
+    t.cy = tile(3, k.ny, k.nx, 8);
+    t.mx = tile(4, k.nx, k.ny, 16);
+    t.sigma = tile(5, k.nz, k.ny, kSigmaRows);
     return t;
 }
 
@@ -1531,12 +1548,12 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
     };
     // the compile-time path of a kernel fixes its tile: 16 z rows (k_vy,
     // k_vx), 16 y rows (k_fz, k_mx), 8 lines (k_cy), kSigmaRows y rows
-    auto len = [&](int n, int tile, int want) { return tile == want ? n : 0; };
     const StepTiles T = step_tiles(k);
+    auto len = [&](int i, int n) { return T.rt[i] ? 0 : n; };
     mark(-1);
     // the runtime path's tiles divide the grid; a compiled length may be
     // ragged (a separate instantiation carries the masks)
-    dispatch_len(len(k.ny, T.vy, 16), [&](auto NN) {
+    dispatch_len(len(0, k.ny), [&](auto NN) {
         constexpr int N = decltype(NN)::value;
         const dim3 grid(cdiv(k.nz, T.vy), k.nx);
         const size_t sm = smem_vyx(k.ny, T.vy);
@@ -1549,7 +1566,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         k_vy<N, false><<<grid, kThreads, sm, st>>>(k, T.vy);
     });
     mark(0);
-    dispatch_len(len(k.nx, T.vx, 16), [&](auto NN) {
+    dispatch_len(len(1, k.nx), [&](auto NN) {
         constexpr int N = decltype(NN)::value;
         const dim3 grid(cdiv(k.nz, T.vx), k.ny);
         const size_t sm = smem_vyx(k.nx, T.vx);
@@ -1562,7 +1579,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         k_vx<N, false><<<grid, kThreads, sm, st>>>(k, T.vx);
     });
     mark(1);
-    dispatch_len(len(k.nz, T.fz, 16), [&](auto NN) {
+    dispatch_len(len(2, k.nz), [&](auto NN) {
         k_fz<decltype(NN)::value><<<dim3(cdiv(k.ny, T.fz), k.nx, 3), kThreads, smem_fz(k, T.fz), st>>>(k, T.fz);
     });
     mark(2);
@@ -1577,20 +1594,20 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         if (tc) {
             launch_cy_tc(k, false, 3, line0, line_end, st);
         } else {
-            dispatch_len(len(k.ny, L, 8), [&](auto NN) {
+            dispatch_len(len(3, k.ny), [&](auto NN) {
                 k_cy<decltype(NN)::value, false><<<dim3(ncy, 3), kCyThreads, smem_cy(k, L, true), st>>>(k, L, line0,
                                                                                                       line_end);
             });
         }
         mark(3);
-        dispatch_len(len(k.nx, Pm, 16), [&](auto NN) {
+        dispatch_len(len(4, k.nx), [&](auto NN) {
             k_mx<decltype(NN)::value><<<dim3(cdiv(k.ny, Pm), nb, 3), kThreads, smem_mx(k, Pm), st>>>(k, Pm, kz0);
         });
         mark(4);
         if (tc) {
             launch_cy_tc(k, true, kNumGxy, line0, line_end, st);
         } else {
-            dispatch_len(len(k.ny, L, 8), [&](auto NN) {
+            dispatch_len(len(3, k.ny), [&](auto NN) {
                 k_cy<decltype(NN)::value, true><<<dim3(ncy, kNumGxy), kCyThreads, smem_cy(k, L), st>>>(k, L, line0,
                                                                                                      line_end);
             });
@@ -1598,7 +1615,7 @@ void launch_step(const KP& k, cudaStream_t st, StepProfile* prof)
         mark(5);
     }
     const int Ps = T.sigma;
-    dispatch_len(len(k.nz, Ps, kSigmaRows), [&](auto NN) {
+    dispatch_len(len(5, k.nz), [&](auto NN) {
         constexpr int N = decltype(NN)::value;
         const dim3 grid(cdiv(k.ny, Ps), k.nx);
         const size_t sm = smem_sigma(k, Ps, sigma_inplace(N), sigma_nod_ok(N));
@@ -1629,8 +1646,32 @@ size_t step_smem_bytes(const KP& k)
     m = std::max(m, smem_mx(k, T.mx));
     // the layout launch_step takes: in place and three groups on the
     // compile-time path, without the z pass's stress buffer at two stages
-    m = std::max(m, smem_sigma(k, T.sigma, ct_length(k.nz), ct_length(k.nz) && k.pz.nst == 2));
+    m = std::max(m, smem_sigma(k, T.sigma, !T.rt[5], !T.rt[5] && k.pz.nst == 2));
     return m;
+}
+
+void step_tile_set(const KP& k, int tiles[kNumTiled], int runtime[kNumTiled])
+{
+    const StepTiles T = step_tiles(k);
+    const int t[kNumTiled] = {T.vy, T.vx, T.fz, T.cy, T.mx, T.sigma};
+    for (int i = 0; i < kNumTiled; ++i) {
+        if (tiles) tiles[i] = t[i];
+        if (runtime) runtime[i] = T.rt[i] ? 1 : 0;
+    }
+}
+
+bool tiles_valid(const KP& k)
+{
+    // the axis each kernel tiles: z rows (k_vy, k_vx), y rows (k_fz, k_mx,
+    // k_sigma); k_cy's lines need not divide anything (a batch's last tile
+    // is partial)
+    const int axis[kNumTiled] = {k.nz, k.nz, k.ny, 0, k.ny, k.ny};
+    for (int i = 0; i < kNumTiled; ++i) {
+        const int t = k.tile_rt[i];
+        if (t == 0) continue;
+        if (t < 2 || t > 32 || (t & 1) || (axis[i] && axis[i] % t)) return false;
+    }
+    return step_smem_bytes(k) <= kMaxSmem;
 }
 
 void launch_coef_build(const KP& k, const float* velp, const float* vels, const float* rho, const float* gp,
@@ -1654,6 +1695,7 @@ void launch_q_derivative(const KP& k_in, int axis, int fwd, int pw, float* out, 
 {
     KP k = k_in;
     k.Hy[0] = k.H[0];  // the forward y pass works in place on the one scratch spectrum
+    k.hz_scale = 0;
     for (int c = 0; c < 3; ++c) k.Yv[c] = nullptr;  // and writes no y derivative
     const int Pz = tile_of(k.ny, 16);
     k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);

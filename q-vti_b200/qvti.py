@@ -56,9 +56,12 @@ class ShotResult(ctypes.Structure):
                 ("device_ms", ctypes.c_float)]
 
 
+NUM_TILES = 6  # k_vy, k_vx, k_fz, k_cy, k_mx, k_sigma (QVTI_TILE_*)
+
+
 class Tuning(ctypes.Structure):
     _fields_ = [("active", ctypes.c_int), ("kz_batch", ctypes.c_int), ("form", ctypes.c_int),
-                ("gcell_steps", ctypes.c_double)]
+                ("gcell_steps", ctypes.c_double), ("tiles", ctypes.c_int * NUM_TILES)]
 
 
 class RtmOpts(ctypes.Structure):
@@ -117,6 +120,9 @@ def lib():
             "qvti_get_stream": (ctypes.c_int, [_V, ctypes.POINTER(_V)]),
             "qvti_set_kz_batch": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_set_form": (ctypes.c_int, [_V, ctypes.c_int]),
+            "qvti_set_tiles": (ctypes.c_int, [_V, _I]),
+            "qvti_get_tiles": (ctypes.c_int, [_V, _I, _I]),
+            "qvti_autotune_tiles": (ctypes.c_int, [_V, ctypes.c_int, _I, _F]),
             "qvti_set_media": (ctypes.c_int, [_V, ctypes.c_int]),
             "qvti_probe_bounded_wait": (ctypes.c_int, [_V, ctypes.c_double]),
             "qvti_set_injection": (ctypes.c_int, [_V, _F, _F, _F, ctypes.c_int]),
@@ -227,6 +233,23 @@ class Simulation:
     def set_form(self, form):
         """FORM_PLAIN or FORM_TC (qvti_set_form)."""
         _check(lib().qvti_set_form(self._h, int(form)), "qvti_set_form")
+
+    def set_tiles(self, tiles):
+        """Per-kernel tiles, NUM_TILES ints, 0 = default (qvti_set_tiles)."""
+        t = (ctypes.c_int * NUM_TILES)(*[int(v) for v in tiles])
+        _check(lib().qvti_set_tiles(self._h, t), "qvti_set_tiles")
+
+    def tiles(self):
+        """(tiles the step launches take, runtime-kernel flags) (qvti_get_tiles)."""
+        t, r = (ctypes.c_int * NUM_TILES)(), (ctypes.c_int * NUM_TILES)()
+        _check(lib().qvti_get_tiles(self._h, t, r), "qvti_get_tiles")
+        return list(t), list(r)
+
+    def autotune_tiles(self, probe_steps=3):
+        """qvti_autotune_tiles: (chosen settings, their ms per kernel)."""
+        b, m = (ctypes.c_int * NUM_TILES)(), (ctypes.c_float * NUM_TILES)()
+        _check(lib().qvti_autotune_tiles(self._h, int(probe_steps), b, m), "qvti_autotune_tiles")
+        return list(b), list(m)
 
     def set_media(self, media):
         """MEDIA_* (qvti_set_media); call before set_model."""
@@ -363,13 +386,13 @@ def simulation_for_case(c, vti=False, device=0):
 
 
 def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=True, device=0, want_state=False,
-             form=FORM_PLAIN, media=MEDIA_VISCOELASTIC):
+             form=FORM_PLAIN, media=MEDIA_VISCOELASTIC, tiles=None):
     """Run a shot described by a case dict (tests/qvti_cases.py conventions).
 
     Returns dict(rec=[3, nt, rn], snaps={k: [3, ...]}, state=[9, ...] or None).
     ``ref_offset`` adds the reference's +10 to s_iz (cuviscoelas_3D.cu:772);
     ``form`` selects the transforms' form (FORM_PLAIN, FORM_TC), ``media``
-    the medium (MEDIA_*)."""
+    the medium (MEDIA_*), ``tiles`` the per-kernel tiles (set_tiles)."""
     nt = int(c["nt"] if nt is None else nt)
     snaps = sorted(int(s) for s in snaps)
     with simulation_for_case(c, vti=vti, device=device) as sim:
@@ -377,6 +400,8 @@ def run_case(c, nt=None, snaps=(), src_type=SRC_FORCE_X, vti=False, ref_offset=T
             sim.set_form(form)
         if media != MEDIA_VISCOELASTIC:
             sim.set_media(media)
+        if tiles is not None:
+            sim.set_tiles(tiles)
         sim.set_model(c["velp"], c["vels"], c["rho"], c["gama_p"], c["gama_s"],
                       c.get("eps") if vti else None, c.get("delta") if vti else None)
         sim.set_receivers(c["r_iz"], c["r_ix"], c["r_iy"])
@@ -456,11 +481,12 @@ def run_batch(requests, max_active=0, mem_budget=0, device=0):
 
 
 def autotune(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, vti=False, max_active=4, probe_steps=8, device=0):
-    """qvti_autotune_ex: (shots in flight, kz batch, form, Gcell-steps/s)."""
+    """qvti_autotune_ex: (shots in flight, kz batch, form, Gcell-steps/s,
+    per-kernel tiles)."""
     cfg = Config(ntx, nty, ntz, pml, dx, dy, dz, dt, f0, 1 if vti else 0, device, 0.0)
     t = Tuning()
     _check(lib().qvti_autotune_ex(ctypes.byref(cfg), max_active, probe_steps, ctypes.byref(t)), "qvti_autotune_ex")
-    return t.active, t.kz_batch, t.form, t.gcell_steps
+    return t.active, t.kz_batch, t.form, t.gcell_steps, list(t.tiles)
 
 
 class Server:

@@ -62,9 +62,10 @@ def test_batch_with_autotuned_concurrency(qvti, alone):
 
 
 def test_autotune_reports_a_setting(qvti):
-    active, kzb, form, rate = qvti.autotune(64, 64, 64, 8, 10.0, 10.0, 10.0, 0.8e-3, 30.0, vti=True, max_active=3,
-                                            probe_steps=4)
+    active, kzb, form, rate, tiles = qvti.autotune(64, 64, 64, 8, 10.0, 10.0, 10.0, 0.8e-3, 30.0, vti=True,
+                                                   max_active=3, probe_steps=4)
     assert 1 <= active <= 3
+    assert len(tiles) == qvti.NUM_TILES and all(t == 0 or t in (2, 4, 8, 16, 32) for t in tiles)
     assert kzb in (33, 17)
     assert form == qvti.FORM_PLAIN  # no tensor-core plan without a 256-point y axis
     assert rate > 0
@@ -73,8 +74,8 @@ def test_autotune_reports_a_setting(qvti):
 def test_autotune_probes_the_tensor_core_form(qvti):
     """A 256-point y axis has both forms; the tuner times each and keeps the
     faster (the plain form unless the tensor-core plan is 2 % faster)."""
-    active, kzb, form, rate = qvti.autotune(32, 256, 32, 6, 10.0, 10.0, 10.0, 0.8e-3, 30.0, vti=False,
-                                            max_active=2, probe_steps=4)
+    active, kzb, form, rate, _ = qvti.autotune(32, 256, 32, 6, 10.0, 10.0, 10.0, 0.8e-3, 30.0, vti=False,
+                                               max_active=2, probe_steps=4)
     assert form in (qvti.FORM_PLAIN, qvti.FORM_TC) and 1 <= active <= 2 and kzb in (17, 9) and rate > 0
 
 
