@@ -433,7 +433,6 @@ extern "C" int qvti_create(const qvti_config* cfg, qvti_sim** out)
     k.err = s->d_err;
     k.form = kFormPlain;
     k.loss_scale = 1.0f;
-    k.hz_scale = 1;
     k.inj[0] = k.inj[1] = k.inj[2] = nullptr;
     k.inj_nt = 0;
 

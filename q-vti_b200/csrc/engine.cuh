@@ -108,11 +108,6 @@ struct KP {
     // where the length has no compiled kernel); > 0 = the runtime kernel
     // with this tile (qvti_set_tiles, checked by tiles_valid)
     int tile_rt[6];
-    // 1: k_cy's forward pass leaves H[c] multiplied by the z shift
-    // multiplier of c's kz-only field over nz (Fz for vz, Bz for vx and vy),
-    // which is what k_sigma's C2R of that field reads; 0: H is left as k_fz
-    // wrote it (the standalone stage entry points)
-    int hz_scale;
 };
 constexpr int kFormPlain = 0, kFormTc = 1;
 constexpr int kNumTiled = 6;

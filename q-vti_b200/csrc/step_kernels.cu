@@ -125,10 +125,7 @@ __global__ void __launch_bounds__(kThreads) k_fz(KP k, int P_rt)
 // reads or writes 16 consecutive points (128 bytes) of one line, so a warp
 // access touches two lines, and the radix-16 shared-memory stages are
 // conflict-free.  The field is H[0..2] (forward) or G[0..26] (inverse), by
-// blockIdx.y.  The forward pass (KP::hz_scale) also leaves each H value it
-// reads multiplied by M(kz) / nz, M the z shift multiplier of the
-// component's kz-only field (Fz for vz, Bz for vx and vy): k_sigma then
-// inverse-transforms that field straight from H.
+// blockIdx.y.
 constexpr int kCyThreads = 128;  // L = 8 lines x 256 points = one radix-16 butterfly per thread
 
 template <int N, bool INV>
@@ -142,31 +139,18 @@ __global__ void __launch_bounds__(kCyThreads) k_cy(KP k, int L_rt, long long lin
     float2* A = tw + n;
     float2* B = A + L * (n + n / 16);
     float2* C = B + L * (n + n / 16);  // forward with Yv: the lines' y spectra, [L][n]
-    float2* hm = C + L * n;            // forward: M(kz) / nz of each line (hz_scale)
     load_table(tw, k.tw_y, n);
+    __syncthreads();
     // forward: H -> Hy (H stays for k_sigma's kz-only fields); inverse: G in
     // place, blockIdx.y over the fields that went through k_mx
     const int c = blockIdx.y;
     const long long first = line0 + (long long)blockIdx.x * L;
     const int lv = (int)min((long long)L, line_end - first);  // lines of the tile inside the batch
-    const bool hs = !INV && k.hz_scale;
-    if (hs) {
-        const float2* M = c == 2 ? k.Fz : k.Bz;
-        const float inv_nz = 1.0f / k.nz;
-        for (int p = threadIdx.x; p < lv; p += blockDim.x) hm[p] = cscale(M[(int)(first + p) / k.nx], inv_nz);
-    }
-    __syncthreads();
     const long long off = first * n;
     const float2* src = (INV ? k.G[c_gxy[c]] : k.H[c]) + off;
     float2* dst = (INV ? k.G[c_gxy[c]] : k.Hy[c]) + off;
-    float2* hsc = k.H[c] + off;  // hs: written where read, by the reading thread
     const bool ydv = !INV && k.Yv[c] != nullptr;
-    auto load = [&](int p, int i) -> float2 {
-        if (p >= lv) return make_float2(0.f, 0.f);
-        const float2 v = src[(long long)p * n + i];
-        if (hs) hsc[(long long)p * n + i] = cmul(v, hm[p]);
-        return v;
-    };
+    auto load = [&](int p, int i) -> float2 { return p < lv ? src[(long long)p * n + i] : make_float2(0.f, 0.f); };
     auto store = [&](int p, int i, float2 v) {
         if (p < lv) dst[(long long)p * n + i] = v;
         if (ydv) C[p * n + i] = v;
@@ -387,14 +371,17 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
     }
     const float axv = k.ax[x], bxv = k.bx[x], axhv = k.axh[x], bxhv = k.bxh[x];
     // where each of the 27 fields comes from: G (x/y passes), Yv (forward y
-    // pass, already scaled) or H, which the forward y pass left multiplied
-    // by the z shift multiplier over nz (Fz for vz, field 7; Bz for vx and
-    // vy, fields 10 and 22)
+    // pass, already scaled) or H times the z shift multiplier (kind 1:
+    // forward, 2: backward)
     __shared__ const float2* s_src[kNumG];
-    for (int o = threadIdx.x; o < kNumG; o += blockDim.x)
+    __shared__ int s_kind[kNumG];
+    for (int o = threadIdx.x; o < kNumG; o += blockDim.x) {
         s_src[o] = is_gz(o) ? k.H[o == 7 ? 2 : o == 10 ? 0 : 1] : is_gy(o) ? k.Yv[o == 4 ? 1 : o == 16 ? 0 : 2] : k.G[o];
+        s_kind[o] = is_gz(o) ? (o == 7 ? 1 : 2) : 0;
+    }
     __syncthreads();
     const int it = *k.d_it;
+    const float inv_nz = 1.0f / n;
     // inv_dt enters only the loss terms (the spectral time derivative of the
     // constant-Q loss operator): their sign and presence follow the medium
     // (k.loss_scale: 1 viscoelastic, 0 dispersion only, -1 Q-compensated)
@@ -470,14 +457,20 @@ __global__ void __launch_bounds__(sigma_threads(N), sigma_min_blocks(N, sigma_no
         //    of field f packed as A + iB (Hermitian extension of the half
         //    spectra; imaginary parts at kz = 0 and nz/2 dropped like a C2R).
         // a kz-only field (is_gz) is M(kz) H(kz) / nz, a ky-only one (is_gy)
-        // Yv: the forward y pass left both so, the values the x and y round
-        // trip (normalised by 1/ntp) would have produced
+        // Yv, which the forward y pass scaled alike: the values the x and y
+        // round trip (normalised by 1/ntp) would have produced
         auto load = [&](int pp, int i) -> float2 {
             const int f = pp / Qp, q = pp - f * Qp, o = o0 + f;
             if (RAG && 2 * q >= yv) return make_float2(0.f, 0.f);
             const int kk = i <= n / 2 ? i : n - i;
             const float4 gg = *reinterpret_cast<const float4*>(s_src[o] + spec(k, kk, x, y0 + 2 * q));
             float2 a = make_float2(gg.x, gg.y), b = make_float2(gg.z, gg.w);
+            const int kind = s_kind[o];
+            if (kind) {
+                const float2 m = cscale(tzs[(kind == 1 ? 0 : n) + kk], inv_nz);
+                a = cmul(a, m);
+                b = cmul(b, m);
+            }
             if (kk == 0 || 2 * kk == n) { a.y = 0.f; b.y = 0.f; }
             if (i > n / 2) { a.y = -a.y; b.y = -b.y; }
             return make_float2(a.x - b.y, a.y + b.x);
@@ -1390,10 +1383,9 @@ int tile_of(int n, int want)
 }
 
 size_t smem_fz(const KP& k, int P) { return sizeof(float2) * (k.nz + 2 * (P / 2) * (k.nz + k.nz / 16)); }
-// fwd: the forward pass's y-spectrum tile and per-line multipliers
-size_t smem_cy(const KP& k, int L, bool fwd = false)
+size_t smem_cy(const KP& k, int L, bool ydv = false)
 {
-    return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16) + (fwd ? (size_t)L * k.ny + L : 0));
+    return sizeof(float2) * (k.ny + 2 * L * (k.ny + k.ny / 16) + (ydv ? (size_t)L * k.ny : 0));
 }
 size_t smem_mx(const KP& k, int P)
 {
@@ -1695,7 +1687,6 @@ void launch_q_derivative(const KP& k_in, int axis, int fwd, int pw, float* out, 
 {
     KP k = k_in;
     k.Hy[0] = k.H[0];  // the forward y pass works in place on the one scratch spectrum
-    k.hz_scale = 0;
     for (int c = 0; c < 3; ++c) k.Yv[c] = nullptr;  // and writes no y derivative
     const int Pz = tile_of(k.ny, 16);
     k_fz<0><<<dim3(k.ny / Pz, k.nx, 1), kThreads, smem_fz(k, Pz), st>>>(k, Pz);

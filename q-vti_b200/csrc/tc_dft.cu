@@ -308,14 +308,6 @@ __global__ void __launch_bounds__(kTcThreads, INV ? 5 : 4) k_cy_tc(KP k, int nfi
             shift_c = c;  // made visible by the next round's barrier
         }
         put_row(Ahi, Alo, t, v);
-        if (!INV && k.hz_scale && p < lv) {
-            // H[c] times M(kz) / nz for k_sigma's kz-only field of c, as
-            // k_cy's forward pass leaves it (line first + p is (kz, x))
-            const float2 m = cscale((c == 2 ? k.Fz : k.Bz)[(int)(first + p) / k.nx], 1.0f / k.nz);
-            float2* h = k.H[c] + (first + p) * kTcN;
-#pragma unroll
-            for (int r = 0; r < 16; ++r) h[j + 16 * r] = cmul(v[r], m);
-        }
         // the next tile's inputs, in flight during this tile's rounds
         const int c_cur = c, lv_cur = lv;
         const int wn = w + gridDim.x;
