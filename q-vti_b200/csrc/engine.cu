@@ -193,6 +193,8 @@ struct Sim {
     int* d_riy = nullptr;
     float* d_rec[3] = {};
     size_t rik_cap = 0, rix_cap = 0, rec_cap = 0;  // element capacities of the buffers above
+    float** d_coefp = nullptr;  // device copy of coef[] (the coefficient build's outputs)
+    size_t coefp_cap = 0;
     double* d_norm = nullptr;
     int* d_bad = nullptr;
     int* d_err = nullptr;  // set by a kernel whose bounded wait gave up
@@ -483,44 +485,51 @@ extern "C" int qvti_destroy(qvti_sim* sim)
     return QVTI_OK;
 }
 
+namespace qvti {
+// The model upload and coefficient build, queued on the simulation's stream.
+// Host arrays are staged in spectrum scratch arrays (G), which hold nothing
+// between steps and are at least ntp floats each, so no device memory is
+// allocated.  sync: return once the host arrays have been read (the
+// contract of qvti_set_model); without it the caller keeps them valid until
+// the stream has passed the upload.
+int set_model_impl(Sim* s, const float* const host[7], int on_device, bool sync)
+{
+    QV_CUDA(cudaSetDevice(s->cfg.device));
+    const size_t bytes = sizeof(float) * s->ntp;
+    const int nin = s->cfg.vti ? 7 : 5;
+    const float* dev[7] = {};
+    if (on_device) {
+        for (int i = 0; i < nin; ++i) dev[i] = host[i];
+    } else {
+        int o = 0;
+        for (int i = 0; i < nin; ++i) {
+            while (is_gz(o)) ++o;  // the kz-only fields have no G array
+            float* stage = reinterpret_cast<float*>(s->kp.G[o++]);
+            QV_CUDA(cudaMemcpyAsync(stage, host[i], bytes, cudaMemcpyHostToDevice, s->st));
+            dev[i] = stage;
+        }
+    }
+    if (s->ensure(&s->d_coefp, &s->coefp_cap, 12)) return g_last_error;
+    QV_CUDA(cudaMemcpyAsync(s->d_coefp, s->coef, sizeof(float*) * 12, cudaMemcpyHostToDevice, s->st));
+    launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
+                      s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, s->kp.w0, s->media == QVTI_MEDIA_LOSSLESS,
+                      s->d_coefp, s->st);
+    launch_mu_rinv(s->kp, dev[2], s->coef + 7, s->st);
+    QV_CUDA(cudaGetLastError());
+    if (sync) QV_CUDA(cudaStreamSynchronize(s->st));
+    s->have_model = true;
+    return QVTI_OK;
+}
+}  // namespace qvti
+
 extern "C" int qvti_set_model(qvti_sim* s, const float* velp, const float* vels, const float* rho, const float* gama_p,
                               const float* gama_s, const float* eps, const float* delta, int on_device)
 {
     using namespace qvti;
     if (!s || !velp || !vels || !rho || !gama_p || !gama_s) return fail(QVTI_ERR_ARG);
     if (s->cfg.vti && (!eps || !delta)) return fail(QVTI_ERR_ARG);
-    QV_CUDA(cudaSetDevice(s->cfg.device));
-    const long long ntp = s->ntp;
-    const size_t bytes = sizeof(float) * ntp;
-    const int nin = s->cfg.vti ? 7 : 5;
     const float* host[7] = {velp, vels, rho, gama_p, gama_s, eps, delta};
-    const float* dev[7] = {};
-    float* tmp[7] = {};
-    if (on_device) {
-        for (int i = 0; i < nin; ++i) dev[i] = host[i];
-    } else {
-        for (int i = 0; i < nin; ++i) {
-            // stream-ordered temporaries: allocating and freeing them does not
-            // synchronise with other simulations' streams
-            QV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&tmp[i]), bytes, s->st));
-            QV_CUDA(cudaMemcpyAsync(tmp[i], host[i], bytes, cudaMemcpyHostToDevice, s->st));
-            dev[i] = tmp[i];
-        }
-    }
-    float** d_coef = nullptr;
-    QV_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d_coef), sizeof(float*) * 12, s->st));
-    QV_CUDA(cudaMemcpyAsync(d_coef, s->coef, sizeof(float*) * 12, cudaMemcpyHostToDevice, s->st));
-    const float w0 = s->kp.w0;
-    launch_coef_build(s->kp, dev[0], dev[1], dev[2], dev[3], dev[4], s->cfg.vti ? dev[5] : nullptr,
-                      s->cfg.vti ? dev[6] : nullptr, s->cfg.vti, w0, s->media == QVTI_MEDIA_LOSSLESS, d_coef, s->st);
-    launch_mu_rinv(s->kp, dev[2], s->coef + 7, s->st);
-    QV_CUDA(cudaGetLastError());
-    QV_CUDA(cudaStreamSynchronize(s->st));
-    QV_CUDA(cudaFreeAsync(d_coef, s->st));
-    for (int i = 0; i < nin; ++i)
-        if (tmp[i]) QV_CUDA(cudaFreeAsync(tmp[i], s->st));
-    s->have_model = true;
-    return QVTI_OK;
+    return set_model_impl(s, host, on_device, true);
 }
 
 extern "C" int qvti_set_source(qvti_sim* s, int type, int s_ix, int s_iy, int s_iz, const float* wavelet, int nt)
@@ -597,10 +606,10 @@ extern "C" int qvti_set_receivers(qvti_sim* s, int r_iz, const int* r_ix, const 
     return QVTI_OK;
 }
 
-extern "C" int qvti_reset(qvti_sim* s)
+namespace qvti {
+// State cleared on the simulation's stream; sync: wait for it.
+int reset_impl(Sim* s, bool sync)
 {
-    using namespace qvti;
-    if (!s) return fail(QVTI_ERR_ARG);
     QV_CUDA(cudaSetDevice(s->cfg.device));
     KP& k = s->kp;
     const size_t b = sizeof(float) * s->ntp;
@@ -618,9 +627,17 @@ extern "C" int qvti_reset(qvti_sim* s)
     QV_CUDA(cudaMemsetAsync(s->d_nonfinite, 0, sizeof(int), s->st));
     for (int c = 0; c < 3; ++c)
         if (s->d_rec[c]) QV_CUDA(cudaMemsetAsync(s->d_rec[c], 0, sizeof(float) * (size_t)s->nt * s->rn, s->st));
-    QV_CUDA(cudaStreamSynchronize(s->st));
+    if (sync) QV_CUDA(cudaStreamSynchronize(s->st));
     s->steps = 0;
     return QVTI_OK;
+}
+}  // namespace qvti
+
+extern "C" int qvti_reset(qvti_sim* s)
+{
+    using namespace qvti;
+    if (!s) return fail(QVTI_ERR_ARG);
+    return reset_impl(s, true);
 }
 
 extern "C" int qvti_step(qvti_sim* s, int nsteps)
@@ -907,11 +924,19 @@ extern "C" int qvti_forward_shot(qvti_sim* s, const float* velp, const float* ve
                                  int src_type, int s_ix, int s_iy, int s_iz, const float* wavelet, int nt, int r_iz,
                                  const int* r_ix, const int* r_iy, int rn, float* rec_vx, float* rec_vy, float* rec_vz)
 {
+    using namespace qvti;
+    if (!s || !velp || !vels || !rho || !gama_p || !gama_s) return fail(QVTI_ERR_ARG);
+    if (s->cfg.vti && (!eps || !delta)) return fail(QVTI_ERR_ARG);
     int rc;
-    if ((rc = qvti_set_model(s, velp, vels, rho, gama_p, gama_s, eps, delta, 0))) return rc;
+    // receivers and source first (each waits for the stream to be idle);
+    // then the model upload and the state clear are queued without a wait,
+    // so the step graphs are built on the host while the copy engines move
+    // the model; the host arrays stay valid until this call returns
     if ((rc = qvti_set_receivers(s, r_iz, r_ix, r_iy, rn))) return rc;
     if ((rc = qvti_set_source(s, src_type, s_ix, s_iy, s_iz, wavelet, nt))) return rc;
-    if ((rc = qvti_reset(s))) return rc;
+    const float* host[7] = {velp, vels, rho, gama_p, gama_s, eps, delta};
+    if ((rc = set_model_impl(s, host, 0, false))) return rc;
+    if ((rc = reset_impl(s, false))) return rc;
     if ((rc = qvti_step(s, nt))) return rc;
     return qvti_get_records(s, rec_vx, rec_vy, rec_vz);
 }
