@@ -155,3 +155,41 @@ def test_void_abi_keeps_its_engine_across_shots(qvti):
         assert created[2] - created[1] == 2, created   # a new engine for the new dt, plus run_case's
     finally:
         L.cuda_Device_free(plan, 1)
+
+
+def test_forward_shot_matches_the_step_by_step_calls(qvti):
+    """qvti_forward_shot queues the model upload and the state clear without
+    waiting and stages the model in spectrum scratch; two shots in a row on
+    one simulation (VTI, the second from another source position, the host
+    model in page-locked memory for one and pageable for the other) equal
+    the same shots through set_model / set_receivers / set_source / reset /
+    step bit for bit."""
+    torch = pytest.importorskip("torch")
+    c = qc.heterogeneous_case(n=(32, 48, 64), pml=6, nt=70, seed=12, src=(16, 24, 30), r_iz=10)
+    rng = np.random.default_rng(3)
+    c["eps"] = (0.05 + 0.2 * rng.random(c["velp"].shape)).astype(np.float32)
+    c["delta"] = (0.1 * rng.random(c["velp"].shape)).astype(np.float32)
+    names = ("velp", "vels", "rho", "gama_p", "gama_s", "eps", "delta")
+    nt, rn = int(c["nt"]), len(c["r_ix"])
+    F = ctypes.POINTER(ctypes.c_float)
+    IP = ctypes.POINTER(ctypes.c_int)
+    rix = np.ascontiguousarray(c["r_ix"], np.int32)
+    riy = np.ascontiguousarray(c["r_iy"], np.int32)
+    rik = np.ascontiguousarray(c["rik"], np.float32)[:nt]
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(c[k], np.float32)).pin_memory() for k in names}
+    pageable = {k: np.ascontiguousarray(c[k], np.float32) for k in names}
+
+    def ptr(a):
+        return ctypes.cast(ctypes.c_void_p(a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data), F)
+
+    with qvti.simulation_for_case(c, vti=True) as sim:
+        for sx, model in ((16, pinned), (11, pageable)):
+            rec = np.zeros((3, nt, rn), np.float32)
+            rc = qvti.lib().qvti_forward_shot(sim._h, *[ptr(model[k]) for k in names], qvti.SRC_FORCE_X, sx,
+                                              int(c["s_iy"]), int(c["s_iz"]) + 10, rik.ctypes.data_as(F), nt,
+                                              int(c["r_iz"]), rix.ctypes.data_as(IP), riy.ctypes.data_as(IP), rn,
+                                              *[rec[i].ctypes.data_as(F) for i in range(3)])
+            assert rc == 0, qvti.lib().qvti_error_string(rc)
+            want = qvti.run_case(dict(c, s_ix=sx), vti=True)["rec"]
+            assert np.abs(want).max() > 0
+            assert np.array_equal(rec, want), "source x %d" % sx
