@@ -77,7 +77,9 @@ long long qvti_sims_created(void);
 /* Set the model: velp, vels, rho, gama_p = atan(1/Qp)/pi, gama_s (and eps,
  * delta when vti) as ntp floats each, host pointers (on_device = 0) or device
  * pointers (on_device = 1).  Builds the constant-Q, C-PML and k-space tables
- * in FP64 on the GPU.  Replaces the model H2D copies and the setup kernels of
+ * in FP64 on the GPU.  Host arrays are staged in the simulation's own
+ * scratch (no device allocation); the call returns once they have been
+ * read.  Replaces the model H2D copies and the setup kernels of
  * cuda_forward_acoustic_3D (cuviscoelas_3D.cu:1179-1230). */
 int qvti_set_model(qvti_sim* sim, const float* velp, const float* vels, const float* rho, const float* gama_p,
                    const float* gama_s, const float* eps, const float* delta, int on_device);
@@ -163,7 +165,11 @@ int qvti_load_state(qvti_sim* sim, const void* host, size_t bytes);
 /* One whole shot with host buffers, synchronous: model upload, setup,
  * nt steps, seismogram download.  The reference-call semantics of
  * cuda_forward_acoustic_3D (Myfunctions.h:77-85, cuviscoelas_3D.cu:1137-1652)
- * with an explicit injection index. rec_* receive nt*rn floats each. */
+ * with an explicit injection index. rec_* receive nt*rn floats each.
+ * Inside the call the model upload and the state clear are queued without
+ * waiting, so the step graphs are built on the host while the model moves;
+ * the results equal qvti_set_model + qvti_set_receivers + qvti_set_source +
+ * qvti_reset + qvti_step + qvti_get_records bit for bit. */
 int qvti_forward_shot(qvti_sim* sim, const float* velp, const float* vels, const float* rho, const float* gama_p,
                       const float* gama_s, const float* eps, const float* delta, int src_type, int s_ix, int s_iy,
                       int s_iz, const float* wavelet, int nt, int r_iz, const int* r_ix, const int* r_iy, int rn,
