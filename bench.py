@@ -567,7 +567,8 @@ def serve_arm(args):
     late = 0.0
     done = queue.Queue()
     res = []
-    with qv.Server(max_active=0, mem_budget=int(150e9)) as srv:
+    policy = qv.SCHED_SMALLEST_FIRST if args.policy == "smallest_first" else qv.SCHED_FIFO
+    with qv.Server(max_active=0, mem_budget=int(150e9), policy=policy) as srv:
         def collect():  # waits in submission order, releasing each request's host arrays
             while True:
                 item = done.get()
@@ -599,6 +600,7 @@ def serve_arm(args):
            "unit": UNIT, "higher_is_better": True, "n_gpus": 1, "dtype": "f32", "data": "synthetic",
            "latency_s": {"p50": q(0.5), "p99": q(0.99), "max": lat[-1]},
            "requests": len(res), "offered_rate_per_s": args.rate, "arrival_window_s": args.duration,
+           "admission": args.policy,
            "max_submit_lag_s": late, "run_s": t_end, "status_ok": ok,
            "config": {"workload": "serving form: Poisson %.1f/s, axes log-uniform 96..384 (x,y), 96..256 (z) "
                                   "rounded to even 5-smooth, nt U[800,3000] x %g, iso/VTI 50/50, layered, pml 20, "
@@ -709,6 +711,8 @@ def main():
     ap.add_argument("--shots", type=int, default=48, help="batch: number of shots")
     ap.add_argument("--nt-scale", type=float, default=0.1, help="batch/serve: fraction of the nominal nt")
     ap.add_argument("--rate", type=float, default=4.0, help="serve: arrivals per second")
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "smallest_first"],
+                    help="serve: admission order of waiting shots")
     ap.add_argument("--duration", type=float, default=60.0, help="serve: arrival window (s)")
     args = ap.parse_args()
     if args.workload == "batch":

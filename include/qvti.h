@@ -352,10 +352,19 @@ typedef struct {
     float device_ms;   /* first to last step of the shot on the GPU (CUDA events) */
 } qvti_shot_result;
 
+/* Admission order of waiting shots.  QVTI_SCHED_FIFO: first submitted,
+ * first admitted.  QVTI_SCHED_SMALLEST_FIRST: the waiting shot with the
+ * fewest cell-steps (ntx nty ntz nt; ties by submission) is admitted next,
+ * which shortens the typical latency of a mix of small and large shots;
+ * the oldest waiting shot is admitted next once smaller ones have passed it
+ * 8 times, so large shots are delayed, not starved. */
+enum { QVTI_SCHED_FIFO = 0, QVTI_SCHED_SMALLEST_FIRST = 1 };
+
 typedef struct {
     int device;        /* CUDA device ordinal                                   */
     size_t mem_budget; /* device bytes the scheduler may hold; 0: 90% of free   */
     int max_active;    /* shots in flight; 0: per grid from qvti_autotune        */
+    int policy;        /* QVTI_SCHED_FIFO or QVTI_SCHED_SMALLEST_FIRST           */
 } qvti_sched_opts;
 
 typedef struct qvti_server qvti_server;

@@ -11,7 +11,8 @@
 //     launched in chunks of kChunk steps
 //     with at most two chunks queued ahead, so a long shot never fills the
 //     launch queue and the scheduler thread stays free;
-//   * shots are admitted first in, first out when a slot and device memory
+//   * shots are admitted first in, first out (or smallest first, with a
+//     bound on how often a shot is passed) when a slot and device memory
 //     are free: an idle pooled simulation of the same grid is reused,
 //     otherwise idle simulations are freed (least recently used first) until
 //     the new one fits the budget;
@@ -42,6 +43,7 @@
 namespace {
 
 constexpr int kChunk = 32;                      // steps per enqueued chunk
+constexpr int kMaxBypass = 8;                   // smallest first: passes before the head goes next
 constexpr long long kCellsInFlight = 1ll << 25;  // default bound: two 256^3 grids
 
 double now_s()
@@ -116,6 +118,7 @@ struct Job {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t chunk[2] = {nullptr, nullptr};
     int nchunk = 0;  // chunks queued and not known finished (0..2)
+    int bypassed = 0;  // times a smaller shot was admitted ahead of it (smallest first)
     int enq = 0;     // steps enqueued
     bool finished = false;  // all steps queued (worker-owned)
     bool ready = false;     // result available (under the server mutex)
@@ -151,6 +154,7 @@ struct qvti_server {
     void top_up(Job* j);
     void finish(Job* j, int status);
     int cap_for(const Job* j, long long active_cells) const;
+    Job* next_waiting() const;
     PoolSim* acquire(const Job* j, bool* blocked);
 };
 
@@ -341,13 +345,27 @@ void qvti_server::finish(Job* j, int status)
 }
 
 // Admit the head of the queue if the slot cap and device memory allow.
+// The waiting shot admission considers next (under mu): the head, or with
+// QVTI_SCHED_SMALLEST_FIRST the one of fewest cell-steps unless the head
+// has been passed kMaxBypass times.
+Job* qvti_server::next_waiting() const
+{
+    Job* head = queue.front();
+    if (opts.policy != QVTI_SCHED_SMALLEST_FIRST || head->bypassed >= kMaxBypass) return head;
+    auto work = [](const Job* j) { return (double)j->shot.ntx * j->shot.nty * j->shot.ntz * j->shot.nt; };
+    Job* best = head;
+    for (Job* j : queue)
+        if (work(j) < work(best)) best = j;  // strict: ties keep submission order
+    return best;
+}
+
 bool qvti_server::admit_one()
 {
     Job* j;
     {
         std::lock_guard<std::mutex> lk(mu);
         if (queue.empty()) return false;
-        j = queue.front();
+        j = next_waiting();
         long long cells = 0;
         for (Job* a : active) cells += (long long)a->shot.ntx * a->shot.nty * a->shot.ntz;
         if (n_active >= cap_for(j, cells)) return false;
@@ -356,8 +374,16 @@ bool qvti_server::admit_one()
     PoolSim* ps = acquire(j, &blocked);
     if (!ps && blocked) return false;
     {
+        // submissions only append: j is still queued, and the shots ahead of
+        // it have been passed once more
         std::lock_guard<std::mutex> lk(mu);
-        queue.pop_front();
+        for (auto it = queue.begin(); it != queue.end(); ++it) {
+            if (*it == j) {
+                queue.erase(it);
+                break;
+            }
+            ++(*it)->bypassed;
+        }
         ++n_active;
     }
     active.push_back(j);
@@ -407,7 +433,9 @@ void qvti_server::loop()
 
 extern "C" int qvti_server_create(const qvti_sched_opts* opts, qvti_server** out)
 {
-    if (!opts || !out || opts->max_active < 0) return QVTI_ERR_ARG;
+    if (!opts || !out || opts->max_active < 0 ||
+        (opts->policy != QVTI_SCHED_FIFO && opts->policy != QVTI_SCHED_SMALLEST_FIRST))
+        return QVTI_ERR_ARG;
     *out = nullptr;
     if (cudaSetDevice(opts->device) != cudaSuccess) return QVTI_ERR_CUDA;
     size_t free_b = 0, total_b = 0;

@@ -68,8 +68,13 @@ class RtmOpts(ctypes.Structure):
     _fields_ = [("media", ctypes.c_int), ("snap_every", ctypes.c_int), ("illum_eps", ctypes.c_float)]
 
 
+SCHED_FIFO = 0            # first submitted, first admitted
+SCHED_SMALLEST_FIRST = 1  # fewest cell-steps first (bounded passing)
+
+
 class SchedOpts(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int), ("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int)]
+    _fields_ = [("device", ctypes.c_int), ("mem_budget", ctypes.c_size_t), ("max_active", ctypes.c_int),
+                ("policy", ctypes.c_int)]
 
 
 _lib = None
@@ -461,20 +466,21 @@ class ShotRequest:
         self.cells = shape[0] * shape[1] * shape[2]
 
 
-def _opts(device, mem_budget, max_active):
+def _opts(device, mem_budget, max_active, policy=SCHED_FIFO):
     o = SchedOpts()
-    o.device, o.mem_budget, o.max_active = int(device), int(mem_budget), int(max_active)
+    o.device, o.mem_budget, o.max_active, o.policy = int(device), int(mem_budget), int(max_active), int(policy)
     return o
 
 
-def run_batch(requests, max_active=0, mem_budget=0, device=0):
+def run_batch(requests, max_active=0, mem_budget=0, device=0, policy=SCHED_FIFO):
     """Run ShotRequests through qvti_run_batch; returns (results, wall_s).
     Records land in each request's ``rec`` ([3, nt, rn])."""
     n = len(requests)
     arr = (Shot * n)(*[r.desc for r in requests])
     res = (ShotResult * n)()
     wall = ctypes.c_double(0)
-    rc = lib().qvti_run_batch(arr, n, ctypes.byref(_opts(device, mem_budget, max_active)), res, ctypes.byref(wall))
+    rc = lib().qvti_run_batch(arr, n, ctypes.byref(_opts(device, mem_budget, max_active, policy)), res,
+                              ctypes.byref(wall))
     _check(rc, "qvti_run_batch")
     return [dict(status=r.status, queue_s=r.queue_s, latency_s=r.latency_s, device_ms=r.device_ms) for r in res], \
         wall.value
@@ -493,10 +499,10 @@ class Server:
     """The continuous serving loop (qvti_server_*): submit shots while others
     run; wait for them by ticket."""
 
-    def __init__(self, max_active=0, mem_budget=0, device=0):
+    def __init__(self, max_active=0, mem_budget=0, device=0, policy=SCHED_FIFO):
         h = _V()
-        _check(lib().qvti_server_create(ctypes.byref(_opts(device, mem_budget, max_active)), ctypes.byref(h)),
-               "qvti_server_create")
+        _check(lib().qvti_server_create(ctypes.byref(_opts(device, mem_budget, max_active, policy)),
+                                        ctypes.byref(h)), "qvti_server_create")
         self.h = h
         self.pending = {}
 

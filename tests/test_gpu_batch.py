@@ -108,6 +108,39 @@ def test_server_admits_while_others_run(qvti, alone):
         assert np.array_equal(reqs[i].rec, alone[i])
 
 
+@pytest.mark.parametrize("policy", ["fifo", "smallest_first"])
+def test_server_admission_policy(qvti, alone, policy):
+    """One shot in flight: while the 64^3 VTI shot (21 M cell-steps) runs, a
+    40^3 shot (6.4 M) and then a 32^3 shot (2.3 M) are queued.  First in,
+    first out finishes them in that order; smallest first admits the 32^3
+    shot ahead of the 40^3 one.  Results stay exact either way."""
+    reqs = _requests(qvti)
+    pol = qvti.SCHED_FIFO if policy == "fifo" else qvti.SCHED_SMALLEST_FIRST
+    with qvti.Server(max_active=1, policy=pol) as srv:
+        t3 = srv.submit(reqs[3])
+        deadline = time.time() + 60.0
+        active = 0
+        while active == 0 and time.time() < deadline:  # until the 64^3 shot is admitted (its set-up and
+            active = srv.load()[1]                     # 80 steps then take milliseconds)
+        assert active == 1
+        t4 = srv.submit(reqs[4])
+        t0 = srv.submit(reqs[0])
+        res = {t: srv.wait(t, timeout=120.0) for t in (t3, t4, t0)}
+    for t, i in ((t3, 3), (t4, 4), (t0, 0)):
+        assert res[t] is not None and res[t]["status"] == 0
+        assert np.array_equal(reqs[i].rec, alone[i])
+    # submitted back to back: the one admitted first finishes first
+    if policy == "fifo":
+        assert res[t4]["latency_s"] < res[t0]["latency_s"], res
+    else:
+        assert res[t0]["latency_s"] < res[t4]["latency_s"], res
+
+
+def test_server_rejects_an_unknown_policy(qvti):
+    with pytest.raises(qvti.QvtiError):
+        qvti.Server(policy=7)
+
+
 def test_server_budget_admits_one_at_a_time(qvti, alone):
     """A budget that holds one 64^3 simulation: shots queue for memory, the
     pool frees idle simulations of other grids, results stay exact."""
